@@ -1,0 +1,216 @@
+/*
+ * sq.h -- C ABI of the B200 batched-query library (libsqcuda.so).
+ *
+ * This is the boundary a host binding links against in place of the
+ * spatial-query crate's `gpu` feature (crates/spatial-query/src/gpu/mod.rs).
+ * Every entry point takes plain pointers and sizes; none takes or returns a
+ * Rust, C++ or torch type. Entry points return an int32 status (SQ_OK = 0);
+ * the message of the last failure on a context is sq_ctx_last_error(). No
+ * entry point unwinds or aborts across the boundary.
+ *
+ * Conventions shared by every query:
+ *   D        the dimension of the uploaded tree (2, 3, 4 or 6).
+ *   ray      origin[D], dir[D] as floats (dir unit length: the crate's
+ *            `Ray::new` normalises on the host, maths/ray.rs:18-23).
+ *   cast     origin[D], dir[D], probe_min[D], probe_max[D]
+ *            (query/shapecast.rs:26-40: the probe box as offsets).
+ *   region   min[D], max[D] (maths/aabb.rs:8-12).
+ *   leaf     the provider leaf index 0..leaf_count; SQ_NO_HIT when none.
+ *   results  bit-identical to the reference CPU path (accel/bvh.rs,
+ *            accel/tlas.rs): the same leaf, the same f32 time of impact, the
+ *            same (toi, leaf) total order (query/hit.rs:77-84).
+ *
+ * Host-buffer entry points copy inputs in and results out on the context's
+ * stream and return when the results are in host memory. The `_d` variants
+ * take device pointers, enqueue on the context's stream and return at once.
+ *
+ * Threading: a context is used by one host thread at a time; uploaded scenes
+ * may be shared by contexts on the same device.
+ */
+#ifndef SQ_H
+#define SQ_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define SQ_OK 0
+#define SQ_ERR_INVALID 1      /* a bad argument: size, pointer, dimension, tree shape */
+#define SQ_ERR_CUDA 2         /* a CUDA runtime failure (message in sq_ctx_last_error) */
+#define SQ_ERR_NO_DEVICE 3    /* no CUDA device (the `headless` -> None case, gpu/mod.rs:308-324) */
+#define SQ_ERR_UNSUPPORTED 4  /* a dimension / narrow-phase pair this build has no kernel for */
+#define SQ_ERR_DEPTH 5        /* the tree is deeper than the traversal stack */
+#define SQ_ERR_CAPACITY 6     /* an output buffer is too small; the needed size is reported */
+#define SQ_ERR_COMPILE 7      /* a consumer narrow phase failed to compile */
+
+#define SQ_NO_HIT 0xFFFFFFFFu /* leaf of a query with no hit */
+#define SQ_NO_SUB 0xFFFFFFFFu /* sub-object `None` (query/hit.rs:36-40) */
+
+/* Built-in narrow phases (the providers' QueryGeometry::test_ray etc.). */
+#define SQ_NARROW_AABB 0        /* leaf = box min[D],max[D]; hit = slab entry (maths/aabb.rs:118-148) */
+#define SQ_NARROW_SPHERE 1      /* leaf = centre[D],radius; near root, far root from inside (tests/differential.rs:61-82) */
+#define SQ_NARROW_SPHERE_NEAR 2 /* leaf = centre[D],radius; near root only (tests/gpu.rs:92-106) */
+#define SQ_NARROW_TRIANGLE 3    /* leaf = v0,v1,v2 (D = 3); Moeller-Trumbore (viewport-lib-query/src/lib.rs:295-320) */
+
+/* Traversal order of nearest queries. */
+#define SQ_ORDER_NEAR_FIRST 0   /* visit the child with the smaller slab entry first (fewest nodes) */
+#define SQ_ORDER_REFERENCE 1    /* the crate's own order (accel/bvh.rs:119-120): replays the CPU step for step */
+
+typedef struct sq_ctx sq_ctx;
+typedef struct sq_bvh sq_bvh;
+
+/* QueryFilter (query/filter.rs:12-29). Honoured when the scene was uploaded
+ * with per-leaf layers: a leaf is accepted when layers[leaf] & layer_mask is
+ * non-zero and leaf != exclude. Without layers every leaf is accepted (the
+ * QueryGeometry::accepts default, query/geometry.rs:95-97). NULL = default. */
+typedef struct sq_filter {
+  uint64_t layer_mask; /* default: all bits */
+  int64_t exclude;     /* a leaf index, or -1 for none */
+} sq_filter;
+
+/* One result per query (GpuHit, gpu/mod.rs:104-114, plus the sub-object).
+ * Any pointer but `leaf` may be NULL to skip that output. */
+typedef struct sq_hits {
+  uint32_t* leaf;       /* [n] SQ_NO_HIT when nothing was hit */
+  float* toi;           /* [n] */
+  uint32_t* sub_object; /* [n] the per-leaf sub-object given at upload, SQ_NO_SUB if none */
+  float* normal;        /* [n*D] */
+  float* point;         /* [n*D] origin + dir * toi, no FMA (maths/ray.rs:33-35) */
+} sq_hits;
+
+/* Bounded sorted hit lists (raycast_all / shapecast_all): count[q] is the full
+ * number of hits, the first min(count[q], k) entries of query q are stored in
+ * hit order at [q*k ...]; entries past that are left untouched. */
+typedef struct sq_hit_lists {
+  uint32_t k;
+  uint32_t* count;      /* [n] */
+  uint32_t* leaf;       /* [n*k] */
+  float* toi;           /* [n*k] */
+  uint32_t* sub_object; /* [n*k] or NULL */
+  float* normal;        /* [n*k*D] or NULL */
+} sq_hit_lists;
+
+/* QueryStats (accel/stats.rs:41-50), summed over the batch. */
+typedef struct sq_query_stats {
+  uint64_t nodes_visited;
+  uint64_t aabb_tests;
+  uint64_t narrow_tests;
+  uint64_t hits;
+} sq_query_stats;
+
+typedef struct sq_bvh_info {
+  int32_t dim;
+  int32_t narrow;
+  uint32_t n_nodes;      /* nodes of the uploaded host tree */
+  uint32_t n_prims;
+  uint32_t max_depth;    /* in nodes (tree.rs:81-99) */
+  uint32_t n_interior;
+  uint64_t device_bytes; /* node records + primitive records + tables */
+  uint32_t node_record_bytes;
+  uint32_t prim_record_bytes;
+} sq_bvh_info;
+
+/* ---- context ---------------------------------------------------------------
+ * Replaces GpuRaycaster::headless / new's device acquisition
+ * (gpu/mod.rs:252-324): returns SQ_ERR_NO_DEVICE when there is no GPU. */
+int32_t sq_version(void);
+int32_t sq_ctx_create(int32_t device, sq_ctx** out);
+int32_t sq_ctx_destroy(sq_ctx* ctx);
+const char* sq_ctx_last_error(const sq_ctx* ctx);
+/* The context's stream (a cudaStream_t); `stream` NULL restores its own. */
+void* sq_ctx_stream(sq_ctx* ctx);
+int32_t sq_ctx_set_stream(sq_ctx* ctx, void* stream);
+int32_t sq_ctx_synchronize(sq_ctx* ctx);
+/* Nearest-query order (SQ_ORDER_*) and persistent-grid blocks per SM (0 = occupancy). */
+int32_t sq_ctx_set_order(sq_ctx* ctx, int32_t order);
+int32_t sq_ctx_set_blocks_per_sm(sq_ctx* ctx, int32_t blocks);
+/* Kernels this context has launched so far. */
+uint64_t sq_ctx_launch_count(const sq_ctx* ctx);
+
+/* ---- host tree build -------------------------------------------------------
+ * tree::build (accel/tree.rs:39-49, 112-163): the median-split tree the
+ * crate's Bvh::build / Tlas::build make, for callers without the Rust crate.
+ * prim_aabbs is n * 2D floats (min, max); outputs need capacity for
+ * max(2n - 1, 0) nodes; node_bounds is n_nodes * 2D. threads <= 0: all cores. */
+int32_t sq_tree_build(int32_t dim, uint32_t n, const float* prim_aabbs, int32_t threads, uint32_t node_capacity,
+                      uint32_t* n_nodes_out, float* node_bounds, uint32_t* child_a, uint32_t* child_b,
+                      uint32_t* prim_count, uint32_t* prim_indices);
+
+/* The world AABB of each built-in leaf (the providers' world_aabb). */
+int32_t sq_prim_aabbs(int32_t dim, int32_t narrow, uint32_t n, const float* prim_data, float* out_aabbs);
+
+/* ---- scene upload (GpuRaycaster::new, gpu/mod.rs:252-303) -------------------
+ * Takes the host tree as tree::Node arrays (accel/tree.rs:21-26; Bvh::nodes
+ * and Bvh::prim_indices, accel/bvh.rs:463-475) and the leaf parameters indexed
+ * by leaf id (prim_stride floats each: 2D boxes, D+1 balls, 9 triangles;
+ * GpuGeometry::prim_data, gpu/mod.rs:86-99). layers (u64 per leaf) and
+ * sub_objects (u32 per leaf) are optional. */
+int32_t sq_bvh_upload(sq_ctx* ctx, int32_t dim, int32_t narrow, uint32_t n_nodes, const float* node_bounds,
+                      const uint32_t* child_a, const uint32_t* child_b, const uint32_t* prim_count, uint32_t n_prims,
+                      const uint32_t* prim_indices, const float* prim_data, uint32_t prim_stride,
+                      const uint64_t* layers, const uint32_t* sub_objects, sq_bvh** out);
+int32_t sq_bvh_destroy(sq_bvh* bvh);
+int32_t sq_bvh_info_get(const sq_bvh* bvh, sq_bvh_info* out);
+
+/* GpuRaycaster::refit (gpu/mod.rs:333-341) with the refit itself on the
+ * device: new leaf parameters (same layout as at upload), then a bottom-up
+ * pass over the fixed topology (tree::refit, accel/tree.rs:54-75). */
+int32_t sq_bvh_refit(sq_ctx* ctx, sq_bvh* bvh, const float* prim_data);
+int32_t sq_bvh_refit_d(sq_ctx* ctx, sq_bvh* bvh, const float* d_prim_data);
+/* Node bounds back in host-tree node order (n_nodes * 2D floats). */
+int32_t sq_bvh_read_bounds(sq_ctx* ctx, const sq_bvh* bvh, float* node_bounds);
+
+/* ---- queries ------------------------------------------------------------------
+ * raycast_nearest: GpuRaycaster::raycast_nearest_batch (gpu/mod.rs:348-463)
+ * and Bvh::raycast_nearest_batch (accel/bvh.rs:134-144). max_toi_per_query
+ * (may be NULL) overrides max_toi per query. stats may be NULL. */
+int32_t sq_raycast_nearest(sq_ctx* ctx, const sq_bvh* bvh, const float* rays, uint32_t n, float max_toi,
+                           const float* max_toi_per_query, const sq_filter* filter, const sq_hits* out,
+                           sq_query_stats* stats);
+int32_t sq_raycast_nearest_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_rays, uint32_t n, float max_toi,
+                             const float* d_max_toi_per_query, const sq_filter* filter, const sq_hits* d_out,
+                             sq_query_stats* stats);
+
+/* raycast_all (accel/bvh.rs:196-259), bounded to k hits per query. */
+int32_t sq_raycast_all(sq_ctx* ctx, const sq_bvh* bvh, const float* rays, uint32_t n, float max_toi,
+                       const float* max_toi_per_query, const sq_filter* filter, const sq_hit_lists* out,
+                       sq_query_stats* stats);
+int32_t sq_raycast_all_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_rays, uint32_t n, float max_toi,
+                         const float* d_max_toi_per_query, const sq_filter* filter, const sq_hit_lists* d_out,
+                         sq_query_stats* stats);
+
+/* raycast_crossings (accel/bvh.rs:261-328): every entry and exit of sphere
+ * leaves; one crossing per hit for the other narrow phases. */
+int32_t sq_raycast_crossings(sq_ctx* ctx, const sq_bvh* bvh, const float* rays, uint32_t n, float max_toi,
+                             const float* max_toi_per_query, const sq_filter* filter, const sq_hit_lists* out);
+int32_t sq_raycast_crossings_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_rays, uint32_t n, float max_toi,
+                               const float* d_max_toi_per_query, const sq_filter* filter, const sq_hit_lists* d_out);
+
+/* shapecast_nearest / shapecast_all (accel/bvh.rs:330-414). The point of a
+ * cast hit is cast.at(toi) (query/shapecast.rs:61-63). */
+int32_t sq_shapecast_nearest(sq_ctx* ctx, const sq_bvh* bvh, const float* casts, uint32_t n, float max_toi,
+                             const float* max_toi_per_query, const sq_filter* filter, const sq_hits* out);
+int32_t sq_shapecast_nearest_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_casts, uint32_t n, float max_toi,
+                               const float* d_max_toi_per_query, const sq_filter* filter, const sq_hits* d_out);
+int32_t sq_shapecast_all(sq_ctx* ctx, const sq_bvh* bvh, const float* casts, uint32_t n, float max_toi,
+                         const float* max_toi_per_query, const sq_filter* filter, const sq_hit_lists* out);
+int32_t sq_shapecast_all_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_casts, uint32_t n, float max_toi,
+                           const float* d_max_toi_per_query, const sq_filter* filter, const sq_hit_lists* d_out);
+
+/* overlap (accel/bvh.rs:416-456) as CSR: offsets[n + 1] (u64, exclusive
+ * prefix) and the leaves of query q at [offsets[q], offsets[q+1]) in ascending
+ * leaf order. When the total exceeds leaf_capacity the call returns
+ * SQ_ERR_CAPACITY with *total and offsets filled and no leaves written. */
+int32_t sq_overlap(sq_ctx* ctx, const sq_bvh* bvh, const float* regions, uint32_t n, const sq_filter* filter,
+                   uint64_t* offsets, uint32_t* leaves, uint64_t leaf_capacity, uint64_t* total);
+int32_t sq_overlap_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_regions, uint32_t n, const sq_filter* filter,
+                     uint64_t* d_offsets, uint32_t* d_leaves, uint64_t leaf_capacity, uint64_t* total);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SQ_H */

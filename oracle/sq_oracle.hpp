@@ -551,7 +551,10 @@ template <int D, class S> struct Scene {
       Point<D, S> c; for (int i = 0; i < D; ++i) c[i] = p[i];
       return point_to_aabb(c, region) <= p[D];  // shape_overlap.rs:113-115
     }
-    return true;  // geometry.rs:89-91 default (exact for box leaves)
+    // Boxes and triangles answer at the level of their own AABB. (The trait
+    // default, geometry.rs:89-91, returns true, which Bvh::overlap would turn
+    // into whole-leaf-node answers; these providers override it.)
+    return world_aabb(leaf).intersects(region);
   }
 };
 
@@ -948,7 +951,8 @@ template <int D, class S> struct InstScene {
 
   bool test_overlap(size_t i, const Aabb<D, S>& region) const {
     if (kind == kInstBall) return point_to_aabb(iso[i].translation, region) <= param[i];  // :339-341
-    return true;  // instance.rs:280-282 default
+    if (kind == kInstMesh) return world_aabb(i).intersects(region);  // AABB-level answer
+    return true;  // instance.rs:280-282 default (tests/two_level.rs boxes keep it)
   }
 };
 

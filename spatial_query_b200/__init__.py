@@ -1,0 +1,531 @@
+"""B200 batched-query path for spatial-query, over the C ABI in include/sq.h.
+
+The host mirror of the crate's `gpu` feature (crates/spatial-query/src/gpu/
+mod.rs) and of the Bvh batch calls it stands in for:
+
+* ``HostBvh.build(geometry)``  -- ``Bvh::build`` (accel/bvh.rs:31-38): the
+  reference median-split tree, built on the host (``sq_tree_build``).
+* ``GpuRaycaster.headless(bvh, geometry)`` / ``.new(ctx, bvh, geometry)`` --
+  ``GpuRaycaster::headless`` / ``new`` (gpu/mod.rs:252-324): ``None`` when
+  there is no CUDA device.
+* ``GpuRaycaster.refit``, ``raycast_nearest_batch`` (gpu/mod.rs:333-463), and
+  the calls the WGSL path never had: ``raycast_all``, ``raycast_crossings``,
+  ``shapecast_nearest``, ``shapecast_all``, ``overlap``.
+
+Every query runs in the CUDA kernels of libsqcuda.so. There is no CPU
+fallback: if the library is missing, importing the binding raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsqcuda.so")
+
+SQ_OK = 0
+SQ_ERR_INVALID = 1
+SQ_ERR_CUDA = 2
+SQ_ERR_NO_DEVICE = 3
+SQ_ERR_UNSUPPORTED = 4
+SQ_ERR_DEPTH = 5
+SQ_ERR_CAPACITY = 6
+SQ_ERR_COMPILE = 7
+NO_HIT = 0xFFFFFFFF
+NO_SUB = 0xFFFFFFFF
+
+NARROW = {"boxes": 0, "aabb": 0, "balls": 1, "sphere": 1, "balls_near": 2, "sphere_near": 2, "tris": 3,
+          "triangle": 3}
+ORDER_NEAR_FIRST = 0
+ORDER_REFERENCE = 1
+
+P = C.c_void_p
+
+
+class SqError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"sq error {code}: {msg}")
+        self.code = code
+
+
+class _Filter(C.Structure):
+    _fields_ = [("layer_mask", C.c_uint64), ("exclude", C.c_int64)]
+
+
+class _Hits(C.Structure):
+    _fields_ = [("leaf", P), ("toi", P), ("sub_object", P), ("normal", P), ("point", P)]
+
+
+class _Lists(C.Structure):
+    _fields_ = [("k", C.c_uint32), ("count", P), ("leaf", P), ("toi", P), ("sub_object", P), ("normal", P)]
+
+
+class _Stats(C.Structure):
+    _fields_ = [("nodes_visited", C.c_uint64), ("aabb_tests", C.c_uint64), ("narrow_tests", C.c_uint64),
+                ("hits", C.c_uint64)]
+
+
+class _Info(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("narrow", C.c_int32), ("n_nodes", C.c_uint32), ("n_prims", C.c_uint32),
+                ("max_depth", C.c_uint32), ("n_interior", C.c_uint32), ("device_bytes", C.c_uint64),
+                ("node_record_bytes", C.c_uint32), ("prim_record_bytes", C.c_uint32)]
+
+
+_lib = None
+
+# Every symbol include/sq.h declares, with its ctypes signature.
+SIGNATURES = {
+    "sq_version": (C.c_int32, []),
+    "sq_ctx_create": (C.c_int32, [C.c_int32, C.POINTER(P)]),
+    "sq_ctx_destroy": (C.c_int32, [P]),
+    "sq_ctx_last_error": (C.c_char_p, [P]),
+    "sq_ctx_stream": (P, [P]),
+    "sq_ctx_set_stream": (C.c_int32, [P, P]),
+    "sq_ctx_synchronize": (C.c_int32, [P]),
+    "sq_ctx_set_order": (C.c_int32, [P, C.c_int32]),
+    "sq_ctx_set_blocks_per_sm": (C.c_int32, [P, C.c_int32]),
+    "sq_ctx_launch_count": (C.c_uint64, [P]),
+    "sq_tree_build": (C.c_int32, [C.c_int32, C.c_uint32, P, C.c_int32, C.c_uint32, P, P, P, P, P, P]),
+    "sq_prim_aabbs": (C.c_int32, [C.c_int32, C.c_int32, C.c_uint32, P, P]),
+    "sq_bvh_upload": (C.c_int32, [P, C.c_int32, C.c_int32, C.c_uint32, P, P, P, P, C.c_uint32, P, P, C.c_uint32,
+                                  P, P, C.POINTER(P)]),
+    "sq_bvh_destroy": (C.c_int32, [P]),
+    "sq_bvh_info_get": (C.c_int32, [P, C.POINTER(_Info)]),
+    "sq_bvh_refit": (C.c_int32, [P, P, P]),
+    "sq_bvh_refit_d": (C.c_int32, [P, P, P]),
+    "sq_bvh_read_bounds": (C.c_int32, [P, P, P]),
+    "sq_raycast_nearest": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P, P]),
+    "sq_raycast_nearest_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P, P]),
+    "sq_raycast_all": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P, P]),
+    "sq_raycast_all_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P, P]),
+    "sq_raycast_crossings": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P]),
+    "sq_raycast_crossings_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P]),
+    "sq_shapecast_nearest": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P]),
+    "sq_shapecast_nearest_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P]),
+    "sq_shapecast_all": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P]),
+    "sq_shapecast_all_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P]),
+    "sq_overlap": (C.c_int32, [P, P, P, C.c_uint32, P, P, P, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "sq_overlap_d": (C.c_int32, [P, P, P, C.c_uint32, P, P, P, C.c_uint64, C.POINTER(C.c_uint64)]),
+}
+
+
+def lib():
+    """The loaded libsqcuda.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with spatial_query_b200/build.py "
+                              "(the query path has no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()  # a torch tensor (device or pinned host)
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+# ---------------------------------------------------------------------------
+# Host tree (Bvh::build) and leaf providers
+# ---------------------------------------------------------------------------
+
+@dataclass
+class Geometry:
+    """A built-in device geometry: the GpuGeometry seam (gpu/mod.rs:86-99).
+
+    ``narrow``: "boxes" (min[D], max[D]), "balls" / "balls_near"
+    (centre[D], radius) or "tris" (v0, v1, v2); ``prims`` is leaf-major.
+    ``layers`` (u64 per leaf) enables the QueryFilter layer test;
+    ``sub_objects`` (u32 per leaf) is returned with each hit."""
+    narrow: str
+    dim: int
+    prims: np.ndarray
+    layers: Optional[np.ndarray] = None
+    sub_objects: Optional[np.ndarray] = None
+
+    def __post_init__(self):
+        self.prims = np.ascontiguousarray(self.prims, dtype=np.float32).reshape(len(self.prims), -1) \
+            if len(self.prims) else np.zeros((0, self.stride), np.float32)
+
+    @property
+    def stride(self) -> int:
+        n = NARROW[self.narrow]
+        return 2 * self.dim if n == 0 else (9 if n == 3 else self.dim + 1)
+
+    @property
+    def leaf_count(self) -> int:
+        return self.prims.shape[0]
+
+    def world_aabbs(self) -> np.ndarray:
+        out = np.empty((self.leaf_count, 2 * self.dim), np.float32)
+        rc = lib().sq_prim_aabbs(self.dim, NARROW[self.narrow], self.leaf_count, _p(self.prims), _p(out))
+        if rc:
+            raise SqError(rc, "sq_prim_aabbs")
+        return out
+
+
+@dataclass
+class HostBvh:
+    """The crate's host tree: tree::Node arrays and the primitive order."""
+    dim: int
+    bounds: np.ndarray
+    child_a: np.ndarray
+    child_b: np.ndarray
+    prim_count: np.ndarray
+    prim_indices: np.ndarray
+
+    @property
+    def node_count(self) -> int:
+        return len(self.child_a)
+
+    @classmethod
+    def build_from_aabbs(cls, dim: int, aabbs: np.ndarray, threads: int = 0) -> "HostBvh":
+        aabbs = _f32(aabbs).reshape(-1, 2 * dim)
+        n = aabbs.shape[0]
+        cap = max(2 * n - 1, 1)
+        b = np.empty((cap, 2 * dim), np.float32)
+        ca = np.empty(cap, np.uint32)
+        cb = np.empty(cap, np.uint32)
+        pc = np.empty(cap, np.uint32)
+        pi = np.empty(max(n, 1), np.uint32)
+        nn = C.c_uint32(0)
+        rc = lib().sq_tree_build(dim, n, _p(aabbs), threads, cap, C.byref(nn), _p(b), _p(ca), _p(cb), _p(pc), _p(pi))
+        if rc:
+            raise SqError(rc, "sq_tree_build")
+        k = nn.value
+        return cls(dim, b[:k].copy(), ca[:k].copy(), cb[:k].copy(), pc[:k].copy(), pi[:n].copy())
+
+    @classmethod
+    def build(cls, geom: Geometry, threads: int = 0) -> "HostBvh":
+        return cls.build_from_aabbs(geom.dim, geom.world_aabbs(), threads)
+
+
+# ---------------------------------------------------------------------------
+# Device context and uploaded scene
+# ---------------------------------------------------------------------------
+
+class Context:
+    """A device, a stream and the persistent-kernel bookkeeping."""
+
+    def __init__(self, device: int = 0):
+        h = P()
+        rc = lib().sq_ctx_create(device, C.byref(h))
+        if rc == SQ_ERR_NO_DEVICE:
+            raise SqError(rc, "no CUDA device")
+        if rc:
+            raise SqError(rc, "sq_ctx_create")
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sq_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def check(self, rc: int, what: str):
+        if rc:
+            raise SqError(rc, f"{what}: {lib().sq_ctx_last_error(self.h).decode()}")
+
+    def set_order(self, order: int):
+        self.check(lib().sq_ctx_set_order(self.h, order), "set_order")
+
+    def set_blocks_per_sm(self, blocks: int):
+        self.check(lib().sq_ctx_set_blocks_per_sm(self.h, blocks), "set_blocks_per_sm")
+
+    def set_stream(self, stream_ptr: int | None):
+        self.check(lib().sq_ctx_set_stream(self.h, stream_ptr), "set_stream")
+
+    @property
+    def stream(self) -> int:
+        return lib().sq_ctx_stream(self.h) or 0
+
+    def synchronize(self):
+        self.check(lib().sq_ctx_synchronize(self.h), "synchronize")
+
+    @property
+    def launch_count(self) -> int:
+        return int(lib().sq_ctx_launch_count(self.h))
+
+
+@dataclass
+class Hits:
+    leaf: np.ndarray
+    toi: np.ndarray
+    normal: Optional[np.ndarray] = None
+    point: Optional[np.ndarray] = None
+    sub_object: Optional[np.ndarray] = None
+    stats: Optional[dict] = None
+
+
+@dataclass
+class HitLists:
+    count: np.ndarray
+    leaf: np.ndarray
+    toi: np.ndarray
+    normal: Optional[np.ndarray] = None
+    sub_object: Optional[np.ndarray] = None
+    stats: Optional[dict] = None
+
+
+def _filter(mask, exclude):
+    if mask is None and exclude is None:
+        return None
+    f = _Filter()
+    f.layer_mask = 0xFFFFFFFFFFFFFFFF if mask is None else mask
+    f.exclude = -1 if exclude is None else exclude
+    return C.byref(f)
+
+
+def _stats_dict(s: _Stats) -> dict:
+    return dict(nodes_visited=s.nodes_visited, aabb_tests=s.aabb_tests, narrow_tests=s.narrow_tests, hits=s.hits)
+
+
+class DeviceBvh:
+    """An uploaded scene: child-pair node records and leaf-ordered primitive
+    records in HBM (sq_bvh_upload)."""
+
+    def __init__(self, ctx: Context, tree: HostBvh, geom: Geometry):
+        if tree.dim != geom.dim:
+            raise ValueError("tree and geometry dimensions differ")
+        self.ctx, self.dim, self.geom = ctx, geom.dim, geom
+        self._layers = None if geom.layers is None else np.ascontiguousarray(geom.layers, dtype=np.uint64)
+        self._sub = None if geom.sub_objects is None else np.ascontiguousarray(geom.sub_objects, dtype=np.uint32)
+        h = P()
+        nn = tree.node_count
+        z = np.zeros(4, np.uint32)
+        ctx.check(lib().sq_bvh_upload(ctx.h, geom.dim, NARROW[geom.narrow], nn,
+                                      _p(tree.bounds if nn else z), _p(tree.child_a if nn else z),
+                                      _p(tree.child_b if nn else z), _p(tree.prim_count if nn else z),
+                                      geom.leaf_count, _p(tree.prim_indices if nn else z),
+                                      _p(geom.prims if geom.leaf_count else z), geom.stride, _p(self._layers),
+                                      _p(self._sub), C.byref(h)), "sq_bvh_upload")
+        self.h = h
+        self.tree = tree
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sq_bvh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def info(self) -> dict:
+        i = _Info()
+        self.ctx.check(lib().sq_bvh_info_get(self.h, C.byref(i)), "info")
+        return {k: getattr(i, k) for k, _ in _Info._fields_}
+
+    def refit(self, prims):
+        prims = _f32(prims)
+        self.ctx.check(lib().sq_bvh_refit(self.ctx.h, self.h, _p(prims)), "refit")
+
+    def refit_d(self, d_prims):
+        self.ctx.check(lib().sq_bvh_refit_d(self.ctx.h, self.h, _p(d_prims)), "refit_d")
+
+    def read_bounds(self) -> np.ndarray:
+        out = np.empty((max(self.tree.node_count, 1), 2 * self.dim), np.float32)
+        self.ctx.check(lib().sq_bvh_read_bounds(self.ctx.h, self.h, _p(out)), "read_bounds")
+        return out[: self.tree.node_count]
+
+    # -- host-buffer queries ---------------------------------------------------
+
+    def _nearest(self, fn, q, width, max_toi, mask, exclude, stats, outputs):
+        q = _f32(q).reshape(-1, width * self.dim)
+        n = q.shape[0]
+        per = np.ndim(max_toi) > 0
+        mt = _f32(max_toi) if per else None
+        h = Hits(np.empty(n, np.uint32), np.empty(n, np.float32))
+        if "normal" in outputs:
+            h.normal = np.empty((n, self.dim), np.float32)
+        if "point" in outputs:
+            h.point = np.empty((n, self.dim), np.float32)
+        if "sub" in outputs:
+            h.sub_object = np.empty(n, np.uint32)
+        s = _Hits(_p(h.leaf), _p(h.toi), _p(h.sub_object), _p(h.normal), _p(h.point))
+        args = [self.ctx.h, self.h, _p(q), n, 0.0 if per else float(max_toi), _p(mt), _filter(mask, exclude),
+                C.byref(s)]
+        st = _Stats() if stats else None
+        if fn == "sq_raycast_nearest":
+            args.append(C.byref(st) if st else None)
+        self.ctx.check(getattr(lib(), fn)(*args), fn)
+        if st:
+            h.stats = _stats_dict(st)
+        return h
+
+    def _lists(self, fn, q, width, max_toi, k, mask, exclude, stats, outputs):
+        q = _f32(q).reshape(-1, width * self.dim)
+        n = q.shape[0]
+        per = np.ndim(max_toi) > 0
+        mt = _f32(max_toi) if per else None
+        h = HitLists(np.empty(n, np.uint32), np.empty((n, k), np.uint32), np.empty((n, k), np.float32))
+        if "normal" in outputs:
+            h.normal = np.empty((n, k, self.dim), np.float32)
+        if "sub" in outputs:
+            h.sub_object = np.empty((n, k), np.uint32)
+        s = _Lists(k, _p(h.count), _p(h.leaf), _p(h.toi), _p(h.sub_object), _p(h.normal))
+        args = [self.ctx.h, self.h, _p(q), n, 0.0 if per else float(max_toi), _p(mt), _filter(mask, exclude),
+                C.byref(s)]
+        st = _Stats() if stats else None
+        if fn == "sq_raycast_all":
+            args.append(C.byref(st) if st else None)
+        self.ctx.check(getattr(lib(), fn)(*args), fn)
+        if st:
+            h.stats = _stats_dict(st)
+        return h
+
+    def raycast_nearest(self, rays, max_toi, mask=None, exclude=None, stats=False,
+                        outputs=("normal", "point", "sub")) -> Hits:
+        return self._nearest("sq_raycast_nearest", rays, 2, max_toi, mask, exclude, stats, outputs)
+
+    def raycast_all(self, rays, max_toi, k=16, mask=None, exclude=None, stats=False,
+                    outputs=("normal", "sub")) -> HitLists:
+        return self._lists("sq_raycast_all", rays, 2, max_toi, k, mask, exclude, stats, outputs)
+
+    def raycast_crossings(self, rays, max_toi, k=16, mask=None, exclude=None, outputs=("normal", "sub")) -> HitLists:
+        return self._lists("sq_raycast_crossings", rays, 2, max_toi, k, mask, exclude, False, outputs)
+
+    def shapecast_nearest(self, casts, max_toi, mask=None, exclude=None, outputs=("normal", "point", "sub")) -> Hits:
+        return self._nearest("sq_shapecast_nearest", casts, 4, max_toi, mask, exclude, False, outputs)
+
+    def shapecast_all(self, casts, max_toi, k=16, mask=None, exclude=None, outputs=("normal", "sub")) -> HitLists:
+        return self._lists("sq_shapecast_all", casts, 4, max_toi, k, mask, exclude, False, outputs)
+
+    def overlap(self, regions, mask=None, exclude=None, capacity=None):
+        """CSR (offsets[n+1] u64, leaves u32), leaves ascending per query."""
+        regions = _f32(regions).reshape(-1, 2 * self.dim)
+        n = regions.shape[0]
+        cap = capacity if capacity is not None else max(4 * n, 1024)
+        while True:
+            offsets = np.empty(n + 1, np.uint64)
+            leaves = np.empty(max(cap, 1), np.uint32)
+            total = C.c_uint64(0)
+            rc = lib().sq_overlap(self.ctx.h, self.h, _p(regions), n, _filter(mask, exclude), _p(offsets),
+                                  _p(leaves), cap, C.byref(total))
+            if rc == SQ_ERR_CAPACITY:
+                cap = int(total.value)
+                continue
+            self.ctx.check(rc, "sq_overlap")
+            return offsets, leaves[: int(total.value)]
+
+    # -- device-buffer queries (torch tensors; async on the context stream) -----
+
+    def raycast_nearest_d(self, d_rays, n, max_toi, d_leaf, d_toi=None, d_normal=None, d_point=None, d_sub=None,
+                          d_max_toi=None, mask=None, exclude=None, stats=False):
+        s = _Hits(_p(d_leaf), _p(d_toi), _p(d_sub), _p(d_normal), _p(d_point))
+        st = _Stats() if stats else None
+        self.ctx.check(lib().sq_raycast_nearest_d(self.ctx.h, self.h, _p(d_rays), n, float(max_toi), _p(d_max_toi),
+                                                  _filter(mask, exclude), C.byref(s),
+                                                  C.byref(st) if st else None), "sq_raycast_nearest_d")
+        return _stats_dict(st) if st else None
+
+    def raycast_all_d(self, d_rays, n, max_toi, k, d_count, d_leaf, d_toi, d_normal=None, d_sub=None,
+                      d_max_toi=None, mask=None, exclude=None):
+        s = _Lists(k, _p(d_count), _p(d_leaf), _p(d_toi), _p(d_sub), _p(d_normal))
+        self.ctx.check(lib().sq_raycast_all_d(self.ctx.h, self.h, _p(d_rays), n, float(max_toi), _p(d_max_toi),
+                                              _filter(mask, exclude), C.byref(s), None), "sq_raycast_all_d")
+
+    def shapecast_nearest_d(self, d_casts, n, max_toi, d_leaf, d_toi=None, d_normal=None, d_point=None, d_sub=None,
+                            d_max_toi=None, mask=None, exclude=None):
+        s = _Hits(_p(d_leaf), _p(d_toi), _p(d_sub), _p(d_normal), _p(d_point))
+        self.ctx.check(lib().sq_shapecast_nearest_d(self.ctx.h, self.h, _p(d_casts), n, float(max_toi),
+                                                    _p(d_max_toi), _filter(mask, exclude), C.byref(s)),
+                       "sq_shapecast_nearest_d")
+
+    def overlap_d(self, d_regions, n, d_offsets, d_leaves, capacity, mask=None, exclude=None) -> int:
+        total = C.c_uint64(0)
+        rc = lib().sq_overlap_d(self.ctx.h, self.h, _p(d_regions), n, _filter(mask, exclude), _p(d_offsets),
+                                _p(d_leaves), capacity, C.byref(total))
+        if rc != SQ_ERR_CAPACITY:
+            self.ctx.check(rc, "sq_overlap_d")
+        return int(total.value)
+
+
+# ---------------------------------------------------------------------------
+# GpuRaycaster: the crate's gpu-feature API (gpu/mod.rs:229-463)
+# ---------------------------------------------------------------------------
+
+@dataclass
+class GpuHit:
+    """One ray's nearest hit (gpu/mod.rs:104-114) plus the sub-object."""
+    leaf: int
+    time_of_impact: float
+    point: np.ndarray
+    normal: np.ndarray
+    sub_object: Optional[int] = None
+
+
+class GpuRaycaster:
+    """Drop-in for ``spatial_query::gpu::GpuRaycaster``."""
+
+    def __init__(self, ctx: Context, bvh: HostBvh, geom: Geometry):
+        self.ctx = ctx
+        self.scene = DeviceBvh(ctx, bvh, geom)
+
+    @classmethod
+    def new(cls, ctx: Context, bvh: HostBvh, geom: Geometry) -> "GpuRaycaster":
+        return cls(ctx, bvh, geom)
+
+    @classmethod
+    def headless(cls, bvh: HostBvh, geom: Geometry, device: int = 0) -> Optional["GpuRaycaster"]:
+        """A raycaster on its own context, or None when no CUDA device exists."""
+        try:
+            ctx = Context(device)
+        except SqError as e:
+            if e.code == SQ_ERR_NO_DEVICE:
+                return None
+            raise
+        return cls(ctx, bvh, geom)
+
+    def refit(self, bvh: HostBvh, geom: Geometry):
+        """New leaf parameters for the same topology; the refit runs on the device."""
+        self.scene.refit(geom.prims)
+
+    def raycast_nearest_batch(self, rays, max_toi: float) -> list:
+        """One Optional[GpuHit] per ray, in ray order (gpu/mod.rs:348)."""
+        rays = _f32(rays).reshape(-1, 2 * self.scene.dim)
+        if rays.shape[0] == 0:
+            return []
+        h = self.scene.raycast_nearest(rays, max_toi)
+        out = []
+        for i in range(rays.shape[0]):
+            if h.leaf[i] == NO_HIT:
+                out.append(None)
+            else:
+                sub = None if h.sub_object[i] == NO_SUB else int(h.sub_object[i])
+                out.append(GpuHit(int(h.leaf[i]), float(h.toi[i]), h.point[i].copy(), h.normal[i].copy(), sub))
+        return out
+
+    # the batch forms of the crate's other queries
+    def raycast_all(self, rays, max_toi, k=16, **kw):
+        return self.scene.raycast_all(rays, max_toi, k, **kw)
+
+    def raycast_crossings(self, rays, max_toi, k=16, **kw):
+        return self.scene.raycast_crossings(rays, max_toi, k, **kw)
+
+    def shapecast_nearest(self, casts, max_toi, **kw):
+        return self.scene.shapecast_nearest(casts, max_toi, **kw)
+
+    def shapecast_all(self, casts, max_toi, k=16, **kw):
+        return self.scene.shapecast_all(casts, max_toi, k, **kw)
+
+    def overlap(self, regions, **kw):
+        return self.scene.overlap(regions, **kw)

@@ -1,0 +1,887 @@
+// C ABI of the batched-query library: contexts, scene upload, refit and the
+// query entry points declared in include/sq.h.
+//
+// The host part of GpuRaycaster (crates/spatial-query/src/gpu/mod.rs:229-535)
+// re-designed for CUDA: a context owns a stream, a ring of work counters for
+// the persistent kernels and a growable staging arena (host-buffer calls
+// reuse it, so a steady stream of same-sized batches allocates nothing);
+// an uploaded scene owns its node and primitive records in HBM.
+#include <cuda_runtime.h>
+
+#include <cub/device/device_scan.cuh>
+#include <cuda/std/functional>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/sq.h"
+#include "traverse.cuh"
+
+namespace sq {
+bool kernel_set_d2(int narrow, KernelSet* out);
+bool kernel_set_d3(int narrow, KernelSet* out);
+bool kernel_set_d4(int narrow, KernelSet* out);
+bool kernel_set_d6(int narrow, KernelSet* out);
+}  // namespace sq
+
+using namespace sq;
+
+namespace {
+
+constexpr uint32_t kCounterSlots = 4096;
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+}  // namespace
+
+struct sq_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int sm_count = 0;
+  int order = SQ_ORDER_NEAR_FIRST;
+  int blocks_per_sm = 0;
+  uint32_t* d_counters = nullptr;
+  uint32_t slot = 0;
+  unsigned long long* d_stats = nullptr;
+  DevBuf arena;
+  uint64_t launches = 0;
+  std::unordered_map<const void*, int> occ;
+};
+
+struct sq_bvh {
+  int device = 0;
+  int dim = 0;
+  int narrow = 0;
+  uint32_t n_nodes = 0, n_prims = 0, n_interior = 0, depth = 0, n_leaves = 0;
+  uint32_t stride = 0;
+  uint32_t root_code = 0;
+  float4* d_nodes = nullptr;
+  float4* d_prims = nullptr;
+  float* d_root = nullptr;
+  uint64_t* d_layers = nullptr;
+  uint32_t* d_sub = nullptr;
+  uint32_t* d_prim_ids = nullptr;
+  RefitLeaf* d_leaves = nullptr;
+  uint32_t* d_parents = nullptr;
+  uint32_t* d_arrivals = nullptr;
+  float* d_refit_in = nullptr;  // staging for host refit data
+  KernelSet ks{};
+  size_t bytes = 0;
+  std::vector<uint32_t> h_iidx;  // host node -> interior record (or kNoHit)
+  std::vector<uint32_t> h_child_a, h_child_b, h_count;
+};
+
+namespace {
+
+int32_t fail(sq_ctx* c, int32_t code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int32_t cuda_fail(sq_ctx* c, const char* what, cudaError_t e) {
+  return fail(c, SQ_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(x)                                          \
+  do {                                                 \
+    cudaError_t e_ = (x);                              \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, #x, e_); \
+  } while (0)
+
+bool kernel_set(int dim, int narrow, KernelSet* out) {
+  switch (dim) {
+    case 2: return kernel_set_d2(narrow, out);
+    case 3: return kernel_set_d3(narrow, out);
+    case 4: return kernel_set_d4(narrow, out);
+    case 6: return kernel_set_d6(narrow, out);
+    default: return false;
+  }
+}
+
+uint32_t stride_of(int dim, int narrow) {
+  switch (narrow) {
+    case SQ_NARROW_AABB: return 2 * dim;
+    case SQ_NARROW_SPHERE:
+    case SQ_NARROW_SPHERE_NEAR: return dim + 1;
+    case SQ_NARROW_TRIANGLE: return 9;
+    default: return 0;
+  }
+}
+
+uint32_t prim_vec(int dim, int narrow) {
+  uint32_t payload = narrow == SQ_NARROW_AABB ? 2 * dim : (narrow == SQ_NARROW_TRIANGLE ? 9 : dim + 1);
+  return (payload + 1 + 3) / 4;
+}
+
+uint32_t node_vec(int dim) { return (4 * dim + 2 + 3) / 4; }
+
+int32_t arena_reserve(sq_ctx* ctx, size_t bytes) {
+  if (ctx->arena.cap >= bytes) return SQ_OK;
+  if (ctx->arena.p) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaFree(ctx->arena.p));
+    ctx->arena.p = nullptr;
+    ctx->arena.cap = 0;
+  }
+  size_t cap = std::max<size_t>(bytes, size_t(1) << 20);
+  CK(cudaMalloc(&ctx->arena.p, cap));
+  ctx->arena.cap = cap;
+  return SQ_OK;
+}
+
+// Carves 256-byte-aligned pieces out of the arena.
+struct Carve {
+  size_t off = 0;
+  size_t take(size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) & ~size_t(255);
+    return o;
+  }
+};
+
+int occupancy(sq_ctx* ctx, const void* fn) {
+  auto it = ctx->occ.find(fn);
+  if (it != ctx->occ.end()) return it->second;
+  int nb = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kThreads, 0) != cudaSuccess || nb < 1) nb = 1;
+  ctx->occ[fn] = nb;
+  return nb;
+}
+
+int32_t launch_persistent(sq_ctx* ctx, const void* fn, QueryParams& p) {
+  uint32_t* ctr = ctx->d_counters + (ctx->slot++ % kCounterSlots);
+  CK(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), ctx->stream));
+  p.counter = ctr;
+  int bps = ctx->blocks_per_sm > 0 ? ctx->blocks_per_sm : occupancy(ctx, fn);
+  uint64_t want = (uint64_t(p.n) + kThreads - 1) / kThreads;
+  uint64_t grid = std::min<uint64_t>(uint64_t(ctx->sm_count) * bps, std::max<uint64_t>(want, 1));
+  void* args[] = {&p};
+  CK(cudaLaunchKernel(fn, dim3(unsigned(grid)), dim3(kThreads), args, 0, ctx->stream));
+  ctx->launches++;
+  return SQ_OK;
+}
+
+void base_params(const sq_bvh* b, const sq_filter* f, QueryParams& p) {
+  std::memset(&p, 0, sizeof(p));
+  p.nodes = b->d_nodes;
+  p.prims = b->d_prims;
+  p.layers = b->d_layers;
+  p.sub = b->d_sub;
+  p.root_box = b->d_root;
+  p.root_code = b->root_code;
+  p.mask = f ? f->layer_mask : ~0ull;
+  p.exclude = f ? f->exclude : -1;
+}
+
+int32_t check_scene(sq_ctx* ctx, const sq_bvh* b) {
+  if (!ctx) return SQ_ERR_INVALID;
+  if (!b) return fail(ctx, SQ_ERR_INVALID, "null scene");
+  if (b->device != ctx->device) return fail(ctx, SQ_ERR_INVALID, "scene and context are on different devices");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, "cudaSetDevice", e);
+  return SQ_OK;
+}
+
+// ---- the query cores (device pointers, enqueue only) -----------------------
+
+int32_t nearest_core(sq_ctx* ctx, const sq_bvh* b, bool cast, const float* d_q, uint32_t n, float max_toi,
+                     const float* d_mt, const sq_filter* f, const sq_hits& o, bool stats) {
+  if (n == 0) return SQ_OK;
+  if (!o.leaf) return fail(ctx, SQ_ERR_INVALID, "null leaf output");
+  if (b->n_nodes == 0) {
+    // Empty tree (gpu/mod.rs:352-354): every query misses.
+    CK(cudaMemsetAsync(o.leaf, 0xFF, size_t(n) * 4, ctx->stream));
+    if (o.toi) CK(cudaMemsetAsync(o.toi, 0, size_t(n) * 4, ctx->stream));
+    if (o.sub_object) CK(cudaMemsetAsync(o.sub_object, 0xFF, size_t(n) * 4, ctx->stream));
+    if (o.normal) CK(cudaMemsetAsync(o.normal, 0, size_t(n) * 4 * b->dim, ctx->stream));
+    if (o.point) CK(cudaMemsetAsync(o.point, 0, size_t(n) * 4 * b->dim, ctx->stream));
+    return SQ_OK;
+  }
+  QueryParams p;
+  base_params(b, f, p);
+  p.queries = d_q;
+  p.max_toi_arr = d_mt;
+  p.max_toi = max_toi;
+  p.n = n;
+  p.out_leaf = o.leaf;
+  p.out_toi = o.toi;
+  p.out_sub = o.sub_object;
+  p.out_normal = o.normal;
+  p.out_point = o.point;
+  const int ref = ctx->order == SQ_ORDER_REFERENCE ? 1 : 0;
+  const void* fn;
+  if (cast) {
+    fn = b->ks.cast_nearest[ref];
+  } else {
+    fn = b->ks.ray_nearest[ref][stats ? 1 : 0];
+    if (stats) p.stats = ctx->d_stats;
+  }
+  return launch_persistent(ctx, fn, p);
+}
+
+int32_t list_core(sq_ctx* ctx, const sq_bvh* b, int kind, const float* d_q, uint32_t n, float max_toi,
+                  const float* d_mt, const sq_filter* f, const sq_hit_lists& o, bool stats) {
+  if (n == 0) return SQ_OK;
+  if (!o.count || (o.k && (!o.leaf || !o.toi))) return fail(ctx, SQ_ERR_INVALID, "null list output");
+  if (b->n_nodes == 0) {
+    CK(cudaMemsetAsync(o.count, 0, size_t(n) * 4, ctx->stream));
+    return SQ_OK;
+  }
+  QueryParams p;
+  base_params(b, f, p);
+  p.queries = d_q;
+  p.max_toi_arr = d_mt;
+  p.max_toi = max_toi;
+  p.n = n;
+  p.k = o.k;
+  p.out_count = o.count;
+  p.out_leaf = o.leaf;
+  p.out_toi = o.toi;
+  p.out_sub = o.sub_object;
+  p.out_normal = o.normal;
+  const void* fn;
+  if (kind == kCastAll) {
+    fn = b->ks.cast_all;
+  } else {
+    p.crossings = kind == 100 ? 1 : 0;
+    fn = b->ks.ray_all[stats ? 1 : 0];
+    if (stats) p.stats = ctx->d_stats;
+  }
+  return launch_persistent(ctx, fn, p);
+}
+
+int32_t stats_begin(sq_ctx* ctx, sq_query_stats* st) {
+  if (st) CK(cudaMemsetAsync(ctx->d_stats, 0, 4 * sizeof(unsigned long long), ctx->stream));
+  return SQ_OK;
+}
+
+int32_t stats_end(sq_ctx* ctx, sq_query_stats* st) {
+  if (!st) return SQ_OK;
+  unsigned long long h[4];
+  CK(cudaMemcpyAsync(h, ctx->d_stats, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  st->nodes_visited = h[0];
+  st->aabb_tests = h[1];
+  st->narrow_tests = h[2];
+  st->hits = h[3];
+  return SQ_OK;
+}
+
+int32_t finish(sq_ctx* ctx) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, "kernel launch", e);
+  return SQ_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+// context
+// ============================================================================
+
+extern "C" int32_t sq_version(void) { return 1; }
+
+extern "C" int32_t sq_ctx_create(int32_t device, sq_ctx** out) {
+  if (!out) return SQ_ERR_INVALID;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+    cudaGetLastError();
+    return SQ_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= count) return SQ_ERR_INVALID;
+  sq_ctx* ctx = new sq_ctx();
+  ctx->device = device;
+  auto bail = [&](cudaError_t e, const char* w) {
+    fprintf(stderr, "sq_ctx_create: %s: %s\n", w, cudaGetErrorString(e));
+    if (ctx->d_counters) cudaFree(ctx->d_counters);
+    if (ctx->d_stats) cudaFree(ctx->d_stats);
+    if (ctx->own) cudaStreamDestroy(ctx->own);
+    delete ctx;
+    return SQ_ERR_CUDA;
+  };
+  cudaError_t e;
+  if ((e = cudaSetDevice(device)) != cudaSuccess) return bail(e, "cudaSetDevice");
+  if ((e = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+  ctx->stream = ctx->own;
+  if ((e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
+    return bail(e, "sm count");
+  if ((e = cudaMalloc(&ctx->d_counters, kCounterSlots * sizeof(uint32_t))) != cudaSuccess) return bail(e, "counters");
+  if ((e = cudaMalloc(&ctx->d_stats, 4 * sizeof(unsigned long long))) != cudaSuccess) return bail(e, "stats");
+  *out = ctx;
+  return SQ_OK;
+}
+
+extern "C" int32_t sq_ctx_destroy(sq_ctx* ctx) {
+  if (!ctx) return SQ_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->own) cudaStreamSynchronize(ctx->own);
+  if (ctx->arena.p) cudaFree(ctx->arena.p);
+  if (ctx->d_counters) cudaFree(ctx->d_counters);
+  if (ctx->d_stats) cudaFree(ctx->d_stats);
+  if (ctx->own) cudaStreamDestroy(ctx->own);
+  delete ctx;
+  return SQ_OK;
+}
+
+extern "C" const char* sq_ctx_last_error(const sq_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+extern "C" void* sq_ctx_stream(sq_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+extern "C" int32_t sq_ctx_set_stream(sq_ctx* ctx, void* stream) {
+  if (!ctx) return SQ_ERR_INVALID;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+  return SQ_OK;
+}
+
+extern "C" int32_t sq_ctx_synchronize(sq_ctx* ctx) {
+  if (!ctx) return SQ_ERR_INVALID;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SQ_OK;
+}
+
+extern "C" int32_t sq_ctx_set_order(sq_ctx* ctx, int32_t order) {
+  if (!ctx || (order != SQ_ORDER_NEAR_FIRST && order != SQ_ORDER_REFERENCE)) return SQ_ERR_INVALID;
+  ctx->order = order;
+  return SQ_OK;
+}
+
+extern "C" int32_t sq_ctx_set_blocks_per_sm(sq_ctx* ctx, int32_t blocks) {
+  if (!ctx || blocks < 0 || blocks > 64) return SQ_ERR_INVALID;
+  ctx->blocks_per_sm = blocks;
+  return SQ_OK;
+}
+
+extern "C" uint64_t sq_ctx_launch_count(const sq_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+// ============================================================================
+// upload / refit
+// ============================================================================
+
+extern "C" int32_t sq_bvh_upload(sq_ctx* ctx, int32_t dim, int32_t narrow, uint32_t n_nodes,
+                                 const float* node_bounds, const uint32_t* child_a, const uint32_t* child_b,
+                                 const uint32_t* prim_count, uint32_t n_prims, const uint32_t* prim_indices,
+                                 const float* prim_data, uint32_t prim_stride, const uint64_t* layers,
+                                 const uint32_t* sub_objects, sq_bvh** out) {
+  if (!ctx || !out) return SQ_ERR_INVALID;
+  *out = nullptr;
+  KernelSet ks;
+  if (!kernel_set(dim, narrow, &ks))
+    return fail(ctx, SQ_ERR_UNSUPPORTED, "no kernels for dim " + std::to_string(dim) + " narrow " +
+                                             std::to_string(narrow));
+  if (prim_stride != stride_of(dim, narrow)) return fail(ctx, SQ_ERR_INVALID, "prim_stride does not match the narrow phase");
+  if (n_prims >= kLeafBit || n_nodes >= kLeafBit) return fail(ctx, SQ_ERR_INVALID, "too many nodes or leaves");
+  if ((n_nodes == 0) != (n_prims == 0)) return fail(ctx, SQ_ERR_INVALID, "empty tree with leaves, or leaves without a tree");
+  if (n_nodes && (!node_bounds || !child_a || !child_b || !prim_count || !prim_indices || !prim_data))
+    return fail(ctx, SQ_ERR_INVALID, "null tree array");
+  CK(cudaSetDevice(ctx->device));
+
+  auto b = std::make_unique<sq_bvh>();
+  b->device = ctx->device;
+  b->dim = dim;
+  b->narrow = narrow;
+  b->n_nodes = n_nodes;
+  b->n_prims = n_prims;
+  b->stride = prim_stride;
+  b->ks = ks;
+  if (n_nodes == 0) {
+    *out = b.release();
+    return SQ_OK;
+  }
+
+  // Validate the topology (children after their parent, leaf ranges inside
+  // the index array) and compute the depth in one reverse pass.
+  std::vector<uint32_t> depth(n_nodes, 1);
+  for (uint32_t i = n_nodes; i-- > 0;) {
+    if (prim_count[i] == 0) {
+      if (child_a[i] <= i || child_b[i] <= i || child_a[i] >= n_nodes || child_b[i] >= n_nodes)
+        return fail(ctx, SQ_ERR_INVALID, "interior node " + std::to_string(i) + " has a child out of order");
+      depth[i] = 1 + std::max(depth[child_a[i]], depth[child_b[i]]);
+    } else if (uint64_t(child_a[i]) + prim_count[i] > n_prims) {
+      return fail(ctx, SQ_ERR_INVALID, "leaf node " + std::to_string(i) + " indexes past the primitives");
+    }
+  }
+  b->depth = depth[0];
+  if (b->depth > uint32_t(kStack)) return fail(ctx, SQ_ERR_DEPTH, "tree depth " + std::to_string(b->depth) + " exceeds the traversal stack");
+  // The leaves must partition the index array and the index array must be a
+  // permutation: every kernel walk of a leaf then ends on its own last
+  // primitive, inside the array.
+  {
+    std::vector<uint8_t> seen(n_prims, 0), covered(n_prims, 0);
+    for (uint32_t k = 0; k < n_prims; ++k) {
+      if (prim_indices[k] >= n_prims || seen[prim_indices[k]])
+        return fail(ctx, SQ_ERR_INVALID, "prim_indices is not a permutation");
+      seen[prim_indices[k]] = 1;
+    }
+    for (uint32_t i = 0; i < n_nodes; ++i) {
+      if (prim_count[i] == 0) continue;
+      for (uint32_t k = child_a[i]; k < child_a[i] + prim_count[i]; ++k) {
+        if (covered[k]) return fail(ctx, SQ_ERR_INVALID, "leaf ranges overlap");
+        covered[k] = 1;
+      }
+    }
+    for (uint32_t k = 0; k < n_prims; ++k)
+      if (!covered[k]) return fail(ctx, SQ_ERR_INVALID, "leaf ranges leave a primitive uncovered");
+  }
+
+  // Interior record numbering (node order) and node codes.
+  b->h_iidx.assign(n_nodes, kNoHit);
+  uint32_t ni = 0;
+  for (uint32_t i = 0; i < n_nodes; ++i)
+    if (prim_count[i] == 0) b->h_iidx[i] = ni++;
+  b->n_interior = ni;
+  auto code = [&](uint32_t i) { return prim_count[i] == 0 ? b->h_iidx[i] : (kLeafBit | child_a[i]); };
+  b->root_code = code(0);
+  b->h_child_a.assign(child_a, child_a + n_nodes);
+  b->h_child_b.assign(child_b, child_b + n_nodes);
+  b->h_count.assign(prim_count, prim_count + n_nodes);
+
+  const int D = dim;
+  const uint32_t NV = node_vec(D), PV = prim_vec(D, narrow);
+  std::vector<float> nodes(size_t(std::max<uint32_t>(ni, 1)) * NV * 4, 0.f);
+  std::vector<uint32_t> parents(std::max<uint32_t>(ni, 1), kNoHit);
+  std::vector<RefitLeaf> leaves;
+  for (uint32_t i = 0; i < n_nodes; ++i) {
+    if (prim_count[i] != 0) {
+      if (i == 0) leaves.push_back(RefitLeaf{child_a[0], prim_count[0], kNoHit, 0});
+      continue;
+    }
+    const uint32_t k = b->h_iidx[i];
+    float* r = nodes.data() + size_t(k) * NV * 4;
+    const uint32_t ch[2] = {child_a[i], child_b[i]};
+    for (int s = 0; s < 2; ++s) {
+      const float* cb = node_bounds + size_t(ch[s]) * 2 * D;
+      for (int j = 0; j < 2 * D; ++j) r[s * 2 * D + j] = cb[j];
+      uint32_t c = code(ch[s]);
+      std::memcpy(&r[4 * D + s], &c, 4);
+      if (prim_count[ch[s]] == 0) parents[b->h_iidx[ch[s]]] = (k << 1) | uint32_t(s);
+      else leaves.push_back(RefitLeaf{child_a[ch[s]], prim_count[ch[s]], (k << 1) | uint32_t(s), 0});
+    }
+  }
+  b->n_leaves = uint32_t(leaves.size());
+
+  // Primitive records in leaf order: payload, then the id (flagged on the
+  // last primitive of each leaf).
+  const uint32_t payload = narrow == SQ_NARROW_AABB ? 2 * D : (narrow == SQ_NARROW_TRIANGLE ? 9 : D + 1);
+  std::vector<float> prims(size_t(n_prims) * PV * 4, 0.f);
+  for (const RefitLeaf& L : leaves) {
+    for (uint32_t j = 0; j < L.count; ++j) {
+      const uint32_t pos = L.first + j;
+      const uint32_t id = prim_indices[pos];
+      float* r = prims.data() + size_t(pos) * PV * 4;
+      std::memcpy(r, prim_data + size_t(id) * prim_stride, payload * 4);
+      uint32_t w = id | (j + 1 == L.count ? kLeafBit : 0u);
+      std::memcpy(&r[payload], &w, 4);
+    }
+  }
+
+  auto up = [&](void** dst, const void* src, size_t bytes) -> int32_t {
+    CK(cudaMalloc(dst, std::max<size_t>(bytes, 16)));
+    if (src && bytes) CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+    b->bytes += bytes;
+    return SQ_OK;
+  };
+  int32_t rc;
+  auto cleanup = [&](int32_t code_) {
+    sq_bvh_destroy(b.release());
+    return code_;
+  };
+  if ((rc = up((void**)&b->d_nodes, nodes.data(), nodes.size() * 4))) return cleanup(rc);
+  if ((rc = up((void**)&b->d_prims, prims.data(), prims.size() * 4))) return cleanup(rc);
+  if ((rc = up((void**)&b->d_root, node_bounds, size_t(2) * D * 4))) return cleanup(rc);
+  if ((rc = up((void**)&b->d_prim_ids, prim_indices, size_t(n_prims) * 4))) return cleanup(rc);
+  if ((rc = up((void**)&b->d_leaves, leaves.data(), leaves.size() * sizeof(RefitLeaf)))) return cleanup(rc);
+  if ((rc = up((void**)&b->d_parents, parents.data(), parents.size() * 4))) return cleanup(rc);
+  if ((rc = up((void**)&b->d_arrivals, nullptr, parents.size() * 4))) return cleanup(rc);
+  if (layers && (rc = up((void**)&b->d_layers, layers, size_t(n_prims) * 8))) return cleanup(rc);
+  if (sub_objects && (rc = up((void**)&b->d_sub, sub_objects, size_t(n_prims) * 4))) return cleanup(rc);
+  *out = b.release();
+  return SQ_OK;
+}
+
+extern "C" int32_t sq_bvh_destroy(sq_bvh* b) {
+  if (!b) return SQ_OK;
+  cudaSetDevice(b->device);
+  void* ptrs[] = {b->d_nodes, b->d_prims, b->d_root, b->d_layers, b->d_sub, b->d_prim_ids,
+                  b->d_leaves, b->d_parents, b->d_arrivals, b->d_refit_in};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  delete b;
+  return SQ_OK;
+}
+
+extern "C" int32_t sq_bvh_info_get(const sq_bvh* b, sq_bvh_info* o) {
+  if (!b || !o) return SQ_ERR_INVALID;
+  o->dim = b->dim;
+  o->narrow = b->narrow;
+  o->n_nodes = b->n_nodes;
+  o->n_prims = b->n_prims;
+  o->max_depth = b->depth;
+  o->n_interior = b->n_interior;
+  o->device_bytes = b->bytes;
+  o->node_record_bytes = node_vec(b->dim) * 16;
+  o->prim_record_bytes = prim_vec(b->dim, b->narrow) * 16;
+  return SQ_OK;
+}
+
+extern "C" int32_t sq_bvh_refit_d(sq_ctx* ctx, sq_bvh* b, const float* d_prim_data) {
+  int32_t rc = check_scene(ctx, b);
+  if (rc) return rc;
+  if (b->n_nodes == 0) return SQ_OK;
+  if (!d_prim_data) return fail(ctx, SQ_ERR_INVALID, "null prim data");
+  CK(cudaMemsetAsync(b->d_arrivals, 0, size_t(std::max<uint32_t>(b->n_interior, 1)) * 4, ctx->stream));
+  RefitParams p;
+  p.nodes = b->d_nodes;
+  p.prims = b->d_prims;
+  p.root_box = b->d_root;
+  p.prim_data = d_prim_data;
+  p.prim_ids = b->d_prim_ids;
+  p.leaves = b->d_leaves;
+  p.parents = b->d_parents;
+  p.arrivals = b->d_arrivals;
+  p.n_leaves = b->n_leaves;
+  p.stride = b->stride;
+  void* args[] = {&p};
+  CK(cudaLaunchKernel(b->ks.refit_leaves, dim3((b->n_leaves + 255) / 256), dim3(256), args, 0, ctx->stream));
+  ctx->launches++;
+  return finish(ctx);
+}
+
+extern "C" int32_t sq_bvh_refit(sq_ctx* ctx, sq_bvh* b, const float* prim_data) {
+  int32_t rc = check_scene(ctx, b);
+  if (rc) return rc;
+  if (b->n_nodes == 0) return SQ_OK;
+  if (!prim_data) return fail(ctx, SQ_ERR_INVALID, "null prim data");
+  size_t bytes = size_t(b->n_prims) * b->stride * 4;
+  if (!b->d_refit_in) CK(cudaMalloc(&b->d_refit_in, bytes));
+  CK(cudaMemcpyAsync(b->d_refit_in, prim_data, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  if ((rc = sq_bvh_refit_d(ctx, b, b->d_refit_in))) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SQ_OK;
+}
+
+extern "C" int32_t sq_bvh_read_bounds(sq_ctx* ctx, const sq_bvh* b, float* node_bounds) {
+  int32_t rc = check_scene(ctx, b);
+  if (rc) return rc;
+  if (b->n_nodes == 0) return SQ_OK;
+  if (!node_bounds) return fail(ctx, SQ_ERR_INVALID, "null output");
+  const int D = b->dim;
+  const uint32_t NV = node_vec(D);
+  std::vector<float> nodes(size_t(std::max<uint32_t>(b->n_interior, 1)) * NV * 4);
+  std::vector<float> root(2 * D);
+  CK(cudaMemcpyAsync(nodes.data(), b->d_nodes, nodes.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(root.data(), b->d_root, root.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  std::memcpy(node_bounds, root.data(), root.size() * 4);
+  for (uint32_t i = 0; i < b->n_nodes; ++i) {
+    if (b->h_count[i] != 0) continue;
+    const float* r = nodes.data() + size_t(b->h_iidx[i]) * NV * 4;
+    std::memcpy(node_bounds + size_t(b->h_child_a[i]) * 2 * D, r, 2 * D * 4);
+    std::memcpy(node_bounds + size_t(b->h_child_b[i]) * 2 * D, r + 2 * D, 2 * D * 4);
+  }
+  return SQ_OK;
+}
+
+// ============================================================================
+// queries: device-pointer entry points
+// ============================================================================
+
+extern "C" int32_t sq_raycast_nearest_d(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, uint32_t n,
+                                        float max_toi, const float* d_mt, const sq_filter* f, const sq_hits* o,
+                                        sq_query_stats* st) {
+  int32_t rc = check_scene(ctx, b);
+  if (rc) return rc;
+  if (!o || (n && !d_rays)) return fail(ctx, SQ_ERR_INVALID, "null argument");
+  if ((rc = stats_begin(ctx, st))) return rc;
+  if ((rc = nearest_core(ctx, b, false, d_rays, n, max_toi, d_mt, f, *o, st != nullptr))) return rc;
+  if ((rc = finish(ctx))) return rc;
+  return stats_end(ctx, st);
+}
+
+extern "C" int32_t sq_shapecast_nearest_d(sq_ctx* ctx, const sq_bvh* b, const float* d_casts, uint32_t n,
+                                          float max_toi, const float* d_mt, const sq_filter* f, const sq_hits* o) {
+  int32_t rc = check_scene(ctx, b);
+  if (rc) return rc;
+  if (!o || (n && !d_casts)) return fail(ctx, SQ_ERR_INVALID, "null argument");
+  if ((rc = nearest_core(ctx, b, true, d_casts, n, max_toi, d_mt, f, *o, false))) return rc;
+  return finish(ctx);
+}
+
+extern "C" int32_t sq_raycast_all_d(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, uint32_t n, float max_toi,
+                                    const float* d_mt, const sq_filter* f, const sq_hit_lists* o,
+                                    sq_query_stats* st) {
+  int32_t rc = check_scene(ctx, b);
+  if (rc) return rc;
+  if (!o || (n && !d_rays)) return fail(ctx, SQ_ERR_INVALID, "null argument");
+  if ((rc = stats_begin(ctx, st))) return rc;
+  if ((rc = list_core(ctx, b, kRayAll, d_rays, n, max_toi, d_mt, f, *o, st != nullptr))) return rc;
+  if ((rc = finish(ctx))) return rc;
+  return stats_end(ctx, st);
+}
+
+extern "C" int32_t sq_raycast_crossings_d(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, uint32_t n,
+                                          float max_toi, const float* d_mt, const sq_filter* f,
+                                          const sq_hit_lists* o) {
+  int32_t rc = check_scene(ctx, b);
+  if (rc) return rc;
+  if (!o || (n && !d_rays)) return fail(ctx, SQ_ERR_INVALID, "null argument");
+  if ((rc = list_core(ctx, b, 100, d_rays, n, max_toi, d_mt, f, *o, false))) return rc;
+  return finish(ctx);
+}
+
+extern "C" int32_t sq_shapecast_all_d(sq_ctx* ctx, const sq_bvh* b, const float* d_casts, uint32_t n,
+                                      float max_toi, const float* d_mt, const sq_filter* f, const sq_hit_lists* o) {
+  int32_t rc = check_scene(ctx, b);
+  if (rc) return rc;
+  if (!o || (n && !d_casts)) return fail(ctx, SQ_ERR_INVALID, "null argument");
+  if ((rc = list_core(ctx, b, kCastAll, d_casts, n, max_toi, d_mt, f, *o, false))) return rc;
+  return finish(ctx);
+}
+
+namespace {
+
+// Overlap on device buffers: count pass, exclusive scan into offsets, total
+// read back, fill pass. `scratch` holds n + 1 u32 counts and the scan's
+// temporary storage (scratch_bytes from overlap_scratch_bytes).
+size_t overlap_scan_temp(uint32_t n) {
+  size_t temp = 0;
+  cub::DeviceScan::ExclusiveScan(nullptr, temp, (const uint32_t*)nullptr, (unsigned long long*)nullptr,
+                                 cuda::std::plus<>{}, 0ull, int(n) + 1);
+  return temp;
+}
+
+int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint32_t n, const sq_filter* f,
+                     uint64_t* d_offsets, uint32_t* d_leaves, uint64_t cap, uint64_t* total, void* scratch,
+                     size_t scratch_bytes) {
+  uint32_t* d_counts = (uint32_t*)scratch;
+  size_t counts_bytes = ((size_t(n) + 1) * 4 + 255) & ~size_t(255);
+  void* temp = (char*)scratch + counts_bytes;
+  size_t temp_bytes = scratch_bytes - counts_bytes;
+  CK(cudaMemsetAsync(d_counts, 0, size_t(n + 1) * 4, ctx->stream));
+  if (b->n_nodes != 0 && n != 0) {
+    QueryParams p;
+    base_params(b, f, p);
+    p.queries = d_regions;
+    p.n = n;
+    p.out_count = d_counts;
+    p.fill = 0;
+    int32_t rc = launch_persistent(ctx, b->ks.overlap, p);
+    if (rc) return rc;
+  }
+  CK(cub::DeviceScan::ExclusiveScan(temp, temp_bytes, d_counts, (unsigned long long*)d_offsets, cuda::std::plus<>{},
+                                    0ull, int(n) + 1, ctx->stream));
+  ctx->launches++;
+  unsigned long long tot = 0;
+  CK(cudaMemcpyAsync(&tot, d_offsets + n, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (total) *total = tot;
+  if (tot > cap) return fail(ctx, SQ_ERR_CAPACITY, "overlap results exceed leaf_capacity");
+  if (tot && b->n_nodes != 0) {
+    QueryParams p;
+    base_params(b, f, p);
+    p.queries = d_regions;
+    p.n = n;
+    p.out_count = d_counts;
+    p.fill = 1;
+    p.csr_offsets = (const unsigned long long*)d_offsets;
+    p.csr_leaves = d_leaves;
+    int32_t rc = launch_persistent(ctx, b->ks.overlap, p);
+    if (rc) return rc;
+  }
+  return SQ_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t sq_overlap_d(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint32_t n,
+                                const sq_filter* f, uint64_t* d_offsets, uint32_t* d_leaves, uint64_t cap,
+                                uint64_t* total) {
+  int32_t rc = check_scene(ctx, b);
+  if (rc) return rc;
+  if (!d_offsets || (n && !d_regions)) return fail(ctx, SQ_ERR_INVALID, "null argument");
+  size_t need = ((size_t(n) + 1) * 4 + 255 & ~size_t(255)) + overlap_scan_temp(n) + 256;
+  if ((rc = arena_reserve(ctx, need))) return rc;
+  if ((rc = overlap_core(ctx, b, d_regions, n, f, d_offsets, d_leaves, cap, total, ctx->arena.p, need))) return rc;
+  if ((rc = finish(ctx))) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SQ_OK;
+}
+
+// ============================================================================
+// queries: host-buffer entry points (copy in, run, copy out, wait)
+// ============================================================================
+
+namespace {
+
+struct HostRun {
+  sq_ctx* ctx;
+  Carve cv;
+  char* base() const { return (char*)ctx->arena.p; }
+};
+
+int32_t h2d(sq_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  return SQ_OK;
+}
+int32_t d2h(sq_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  if (dst && bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  return SQ_OK;
+}
+
+int32_t host_nearest(sq_ctx* ctx, const sq_bvh* b, bool cast, const float* q, uint32_t n, float max_toi,
+                     const float* mt, const sq_filter* f, const sq_hits* o, sq_query_stats* st) {
+  int32_t rc = check_scene(ctx, b);
+  if (rc) return rc;
+  if (!o || !o->leaf || (n && !q)) return fail(ctx, SQ_ERR_INVALID, "null argument");
+  if (n == 0) {
+    if (st) *st = sq_query_stats{0, 0, 0, 0};
+    return SQ_OK;
+  }
+  const int D = b->dim;
+  const size_t qb = size_t(n) * (cast ? 4 : 2) * D * 4;
+  Carve cv;
+  size_t o_q = cv.take(qb), o_mt = mt ? cv.take(size_t(n) * 4) : 0;
+  size_t o_leaf = cv.take(size_t(n) * 4), o_toi = o->toi ? cv.take(size_t(n) * 4) : 0;
+  size_t o_sub = o->sub_object ? cv.take(size_t(n) * 4) : 0;
+  size_t o_nrm = o->normal ? cv.take(size_t(n) * D * 4) : 0;
+  size_t o_pt = o->point ? cv.take(size_t(n) * D * 4) : 0;
+  if ((rc = arena_reserve(ctx, cv.off))) return rc;
+  char* base = (char*)ctx->arena.p;
+  if ((rc = h2d(ctx, base + o_q, q, qb))) return rc;
+  if (mt && (rc = h2d(ctx, base + o_mt, mt, size_t(n) * 4))) return rc;
+  sq_hits dh;
+  dh.leaf = (uint32_t*)(base + o_leaf);
+  dh.toi = o->toi ? (float*)(base + o_toi) : nullptr;
+  dh.sub_object = o->sub_object ? (uint32_t*)(base + o_sub) : nullptr;
+  dh.normal = o->normal ? (float*)(base + o_nrm) : nullptr;
+  dh.point = o->point ? (float*)(base + o_pt) : nullptr;
+  if ((rc = stats_begin(ctx, cast ? nullptr : st))) return rc;
+  if ((rc = nearest_core(ctx, b, cast, (const float*)(base + o_q), n, max_toi,
+                         mt ? (const float*)(base + o_mt) : nullptr, f, dh, st && !cast)))
+    return rc;
+  if ((rc = finish(ctx))) return rc;
+  if ((rc = d2h(ctx, o->leaf, dh.leaf, size_t(n) * 4))) return rc;
+  if ((rc = d2h(ctx, o->toi, dh.toi, size_t(n) * 4))) return rc;
+  if ((rc = d2h(ctx, o->sub_object, dh.sub_object, size_t(n) * 4))) return rc;
+  if ((rc = d2h(ctx, o->normal, dh.normal, size_t(n) * D * 4))) return rc;
+  if ((rc = d2h(ctx, o->point, dh.point, size_t(n) * D * 4))) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (!cast) return stats_end(ctx, st);
+  return SQ_OK;
+}
+
+int32_t host_list(sq_ctx* ctx, const sq_bvh* b, int kind, const float* q, uint32_t n, float max_toi,
+                  const float* mt, const sq_filter* f, const sq_hit_lists* o, sq_query_stats* st) {
+  int32_t rc = check_scene(ctx, b);
+  if (rc) return rc;
+  if (!o || !o->count || (n && !q) || (n && o->k && (!o->leaf || !o->toi)))
+    return fail(ctx, SQ_ERR_INVALID, "null argument");
+  if (n == 0) {
+    if (st) *st = sq_query_stats{0, 0, 0, 0};
+    return SQ_OK;
+  }
+  const int D = b->dim;
+  const bool cast = kind == kCastAll;
+  const size_t qb = size_t(n) * (cast ? 4 : 2) * D * 4;
+  const size_t nk = size_t(n) * o->k;
+  Carve cv;
+  size_t o_q = cv.take(qb), o_mt = mt ? cv.take(size_t(n) * 4) : 0;
+  size_t o_cnt = cv.take(size_t(n) * 4);
+  size_t o_leaf = cv.take(nk * 4), o_toi = cv.take(nk * 4);
+  size_t o_sub = o->sub_object ? cv.take(nk * 4) : 0;
+  size_t o_nrm = o->normal ? cv.take(nk * D * 4) : 0;
+  if ((rc = arena_reserve(ctx, cv.off))) return rc;
+  char* base = (char*)ctx->arena.p;
+  if ((rc = h2d(ctx, base + o_q, q, qb))) return rc;
+  if (mt && (rc = h2d(ctx, base + o_mt, mt, size_t(n) * 4))) return rc;
+  sq_hit_lists dl;
+  dl.k = o->k;
+  dl.count = (uint32_t*)(base + o_cnt);
+  dl.leaf = (uint32_t*)(base + o_leaf);
+  dl.toi = (float*)(base + o_toi);
+  dl.sub_object = o->sub_object ? (uint32_t*)(base + o_sub) : nullptr;
+  dl.normal = o->normal ? (float*)(base + o_nrm) : nullptr;
+  // Entries past min(count, k) are unspecified; give them a defined value
+  // in host-buffer calls so callers comparing whole buffers see no garbage.
+  CK(cudaMemsetAsync(dl.leaf, 0xFF, nk * 4, ctx->stream));
+  CK(cudaMemsetAsync(dl.toi, 0, nk * 4, ctx->stream));
+  if (dl.sub_object) CK(cudaMemsetAsync(dl.sub_object, 0xFF, nk * 4, ctx->stream));
+  if (dl.normal) CK(cudaMemsetAsync(dl.normal, 0, nk * D * 4, ctx->stream));
+  if ((rc = stats_begin(ctx, st))) return rc;
+  if ((rc = list_core(ctx, b, kind, (const float*)(base + o_q), n, max_toi, mt ? (const float*)(base + o_mt) : nullptr,
+                      f, dl, st != nullptr)))
+    return rc;
+  if ((rc = finish(ctx))) return rc;
+  if ((rc = d2h(ctx, o->count, dl.count, size_t(n) * 4))) return rc;
+  if ((rc = d2h(ctx, o->leaf, dl.leaf, nk * 4))) return rc;
+  if ((rc = d2h(ctx, o->toi, dl.toi, nk * 4))) return rc;
+  if ((rc = d2h(ctx, o->sub_object, dl.sub_object, nk * 4))) return rc;
+  if ((rc = d2h(ctx, o->normal, dl.normal, nk * D * 4))) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return stats_end(ctx, st);
+}
+
+}  // namespace
+
+extern "C" int32_t sq_raycast_nearest(sq_ctx* ctx, const sq_bvh* b, const float* rays, uint32_t n, float max_toi,
+                                      const float* mt, const sq_filter* f, const sq_hits* o, sq_query_stats* st) {
+  return host_nearest(ctx, b, false, rays, n, max_toi, mt, f, o, st);
+}
+
+extern "C" int32_t sq_shapecast_nearest(sq_ctx* ctx, const sq_bvh* b, const float* casts, uint32_t n,
+                                        float max_toi, const float* mt, const sq_filter* f, const sq_hits* o) {
+  return host_nearest(ctx, b, true, casts, n, max_toi, mt, f, o, nullptr);
+}
+
+extern "C" int32_t sq_raycast_all(sq_ctx* ctx, const sq_bvh* b, const float* rays, uint32_t n, float max_toi,
+                                  const float* mt, const sq_filter* f, const sq_hit_lists* o, sq_query_stats* st) {
+  return host_list(ctx, b, kRayAll, rays, n, max_toi, mt, f, o, st);
+}
+
+extern "C" int32_t sq_raycast_crossings(sq_ctx* ctx, const sq_bvh* b, const float* rays, uint32_t n,
+                                        float max_toi, const float* mt, const sq_filter* f, const sq_hit_lists* o) {
+  return host_list(ctx, b, 100, rays, n, max_toi, mt, f, o, nullptr);
+}
+
+extern "C" int32_t sq_shapecast_all(sq_ctx* ctx, const sq_bvh* b, const float* casts, uint32_t n, float max_toi,
+                                    const float* mt, const sq_filter* f, const sq_hit_lists* o) {
+  return host_list(ctx, b, kCastAll, casts, n, max_toi, mt, f, o, nullptr);
+}
+
+extern "C" int32_t sq_overlap(sq_ctx* ctx, const sq_bvh* b, const float* regions, uint32_t n, const sq_filter* f,
+                              uint64_t* offsets, uint32_t* leaves, uint64_t cap, uint64_t* total) {
+  int32_t rc = check_scene(ctx, b);
+  if (rc) return rc;
+  if (!offsets || (n && !regions)) return fail(ctx, SQ_ERR_INVALID, "null argument");
+  const int D = b->dim;
+  const size_t rb = size_t(n) * 2 * D * 4;
+  const size_t scan = ((size_t(n) + 1) * 4 + 255 & ~size_t(255)) + overlap_scan_temp(n) + 256;
+  Carve cv;
+  size_t o_r = cv.take(rb), o_off = cv.take((size_t(n) + 1) * 8), o_lv = cv.take(std::max<uint64_t>(cap, 1) * 4);
+  size_t o_scr = cv.take(scan);
+  if ((rc = arena_reserve(ctx, cv.off))) return rc;
+  char* base = (char*)ctx->arena.p;
+  if ((rc = h2d(ctx, base + o_r, regions, rb))) return rc;
+  uint64_t tot = 0;
+  rc = overlap_core(ctx, b, (const float*)(base + o_r), n, f, (uint64_t*)(base + o_off), (uint32_t*)(base + o_lv), cap,
+                    &tot, base + o_scr, scan);
+  if (total) *total = tot;
+  if (rc && rc != SQ_ERR_CAPACITY) return rc;
+  int32_t rc2;
+  if ((rc2 = d2h(ctx, offsets, base + o_off, (size_t(n) + 1) * 8))) return rc2;
+  if (rc == SQ_OK && (rc2 = d2h(ctx, leaves, base + o_lv, tot * 4))) return rc2;
+  CK(cudaStreamSynchronize(ctx->stream));
+  if ((rc2 = finish(ctx))) return rc2;
+  return rc;
+}

@@ -1,0 +1,589 @@
+// Persistent, warp-pulled BVH traversal kernels for sm_100a.
+//
+// Replaces the WGSL `main` of crates/spatial-query/src/gpu/mod.rs:159-226 (one
+// invocation per ray, 48-byte nodes, no ordering) with:
+//  * a child-pair node record: an interior node holds both children's boxes
+//    and codes in 16-byte vectors (64 B at D = 3), so one record fetch tests
+//    two boxes;
+//  * a persistent grid (a multiple of the SM count) whose warps pull batches
+//    of 32 queries from an atomic counter, so uneven per-query work balances;
+//  * a per-thread traversal stack in shared memory ([depth][thread], so
+//    consecutive lanes hit consecutive banks), each entry carrying the child's
+//    slab entry so it can be re-checked exactly against the shrunk limit when
+//    popped;
+//  * near-first child ordering for nearest queries, or the reference's own
+//    order (push child_a, then child_b, pop child_b first; accel/bvh.rs:119-120)
+//    when REF is set, which replays the CPU decisions one for one.
+//
+// Node code: an interior record index, or kLeafBit | the first position of the
+// leaf's primitives in the leaf-ordered primitive array. The last primitive of
+// a leaf carries kLeafBit in its id word.
+#pragma once
+
+#include "sq_math.cuh"
+
+namespace sq {
+
+enum Narrow : int { kNarrowAabb = 0, kNarrowSphere = 1, kNarrowSphereNear = 2, kNarrowTri = 3 };
+enum QKind : int { kRayNearest = 0, kRayAll = 1, kCastNearest = 2, kCastAll = 3, kOverlap = 4 };
+
+constexpr int kThreads = 128;
+constexpr int kStack = 32;
+
+template <int D> struct NodeLayout {
+  static constexpr int words = 4 * D + 2;  // a.lo a.hi b.lo b.hi code_a code_b
+  static constexpr int vec = (words + 3) / 4;
+};
+
+template <int D, int N> struct PrimLayout {
+  static constexpr int payload = (N == kNarrowAabb) ? 2 * D : (N == kNarrowTri ? 9 : D + 1);
+  static constexpr int id_word = payload;
+  static constexpr int vec = (payload + 1 + 3) / 4;
+};
+
+template <int K> struct QueryLayout {
+  // floats per query record: rays o,d; casts o,d,probe.min,probe.max; regions lo,hi
+};
+
+struct QueryParams {
+  const float4* __restrict__ nodes;
+  const float4* __restrict__ prims;
+  const uint64_t* __restrict__ layers;
+  const uint32_t* __restrict__ sub;
+  const float* __restrict__ queries;
+  const float* __restrict__ max_toi_arr;
+  uint32_t* counter;
+  uint32_t* out_leaf;
+  float* out_toi;
+  uint32_t* out_sub;
+  float* out_normal;
+  float* out_point;
+  uint32_t* out_count;
+  const unsigned long long* csr_offsets;
+  uint32_t* csr_leaves;
+  unsigned long long* stats;
+  uint32_t* query_stats;  // optional per-query counters [n][4] (u32)
+  unsigned long long mask;
+  long long exclude;
+  const float* root_box;  // min[D], max[D] of the root (device memory: refit updates it)
+  float max_toi;
+  uint32_t root_code;
+  uint32_t n;
+  uint32_t k;
+  int crossings;
+  int fill;
+};
+
+__device__ __forceinline__ bool accepts(const QueryParams& p, uint32_t id) {
+  if (!p.layers) return true;
+  if (p.exclude >= 0 && (unsigned long long)p.exclude == id) return false;
+  return (__ldg(p.layers + id) & p.mask) != 0ull;
+}
+
+template <int NV> __device__ __forceinline__ void load_vec(const float4* __restrict__ src, float* dst) {
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    float4 v = __ldg(src + j);
+    dst[4 * j + 0] = v.x;
+    dst[4 * j + 1] = v.y;
+    dst[4 * j + 2] = v.z;
+    dst[4 * j + 3] = v.w;
+  }
+}
+
+// One primitive's ray test (QueryGeometry::test_ray for the built-in providers).
+template <int D, int N>
+__device__ __forceinline__ bool narrow_ray(const float* rec, const RayPre<D>& r, float max_toi, float& t, float* n) {
+  if constexpr (N == kNarrowAabb) {
+    int axis;
+    if (!slab<D>(r, rec, rec + D, max_toi, t, axis)) return false;
+    entry_normal<D>(r.d, axis, n);
+    return true;
+  } else if constexpr (N == kNarrowSphere || N == kNarrowSphereNear) {
+    return ray_ball<D, N == kNarrowSphere>(r.o, r.d, rec, rec[D], max_toi, t, n);
+  } else {
+    if (!ray_triangle(r.o, r.d, rec, rec + 3, rec + 6, t)) return false;
+    if (t > max_toi) return false;
+    tri_normal(rec, rec + 3, rec + 6, n);
+    return true;
+  }
+}
+
+// One primitive's swept-probe test (QueryGeometry::test_shape_cast).
+template <int D, int N>
+__device__ __forceinline__ bool narrow_cast(const float* rec, const RayPre<D>& r, const float* pmin, const float* pmax,
+                                            float max_toi, float& t, float* n) {
+  if constexpr (N == kNarrowAabb) {
+    int axis;
+    if (!slab_grown<D>(r, rec, rec + D, pmin, pmax, max_toi, t, axis)) return false;
+    entry_normal<D>(r.d, axis, n);
+    return true;
+  } else if constexpr (N == kNarrowSphere || N == kNarrowSphereNear) {
+    return ray_ball<D, N == kNarrowSphere>(r.o, r.d, rec, fadd(rec[D], pmax[0]), max_toi, t, n);
+  } else {
+    float lo[3], hi[3];
+    tri_aabb(rec, rec + 3, rec + 6, lo, hi);
+    int axis;
+    if (!slab_grown<3>(r, lo, hi, pmin, pmax, max_toi, t, axis)) return false;
+    entry_normal<3>(r.d, axis, n);
+    return true;
+  }
+}
+
+// One primitive's overlap test (QueryGeometry::test_overlap): the box itself,
+// point_to_aabb <= radius for balls (tests/shape_overlap.rs:59-72,113-115),
+// the triangle's AABB for triangles.
+template <int D, int N>
+__device__ __forceinline__ bool narrow_overlap(const float* rec, const float* qlo, const float* qhi) {
+  if constexpr (N == kNarrowAabb) {
+    return box_overlap<D>(rec, rec + D, qlo, qhi);
+  } else if constexpr (N == kNarrowSphere || N == kNarrowSphereNear) {
+    float d2 = 0.f;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      float c = rec[i];
+      float v = (c < qlo[i]) ? fsub(qlo[i], c) : ((c > qhi[i]) ? fsub(c, qhi[i]) : 0.f);
+      d2 = fadd(d2, fmul(v, v));
+    }
+    return fsqrt(d2) <= rec[D];
+  } else {
+    float lo[3], hi[3];
+    tri_aabb(rec, rec + 3, rec + 6, lo, hi);
+    return box_overlap<3>(lo, hi, qlo, qhi);
+  }
+}
+
+// Sorted insertion into query q's bounded hit list (hit_ordering, stable:
+// an equal key goes after the entries already present).
+template <int D>
+__device__ __forceinline__ void list_insert(const QueryParams& p, uint32_t q, uint32_t& count, float t, uint32_t leaf,
+                                            const float* n) {
+  const uint32_t k = p.k;
+  uint32_t m = count < k ? count : k;
+  ++count;
+  if (k == 0) return;
+  const size_t base = size_t(q) * k;
+  if (m == k) {
+    if (!hit_before(t, leaf, p.out_toi[base + k - 1], p.out_leaf[base + k - 1])) return;
+    m = k - 1;
+  }
+  uint32_t j = m;
+  while (j > 0 && hit_before(t, leaf, p.out_toi[base + j - 1], p.out_leaf[base + j - 1])) {
+    p.out_toi[base + j] = p.out_toi[base + j - 1];
+    p.out_leaf[base + j] = p.out_leaf[base + j - 1];
+    if (p.out_sub) p.out_sub[base + j] = p.out_sub[base + j - 1];
+    if (p.out_normal)
+#pragma unroll
+      for (int i = 0; i < D; ++i) p.out_normal[(base + j) * D + i] = p.out_normal[(base + j - 1) * D + i];
+    --j;
+  }
+  p.out_toi[base + j] = t;
+  p.out_leaf[base + j] = leaf;
+  if (p.out_sub) p.out_sub[base + j] = p.sub ? __ldg(p.sub + leaf) : kNoHit;
+  if (p.out_normal)
+#pragma unroll
+    for (int i = 0; i < D; ++i) p.out_normal[(base + j) * D + i] = n[i];
+}
+
+template <int D, int N, int K, bool REF, bool STATS>
+__device__ __forceinline__ void run_query(const QueryParams& p, uint32_t q, int tid, uint32_t (*s_code)[kThreads],
+                                          float (*s_t)[kThreads], unsigned long long& c_vis,
+                                          unsigned long long& c_nar, unsigned long long& c_hit) {
+  constexpr bool kNearest = (K == kRayNearest || K == kCastNearest);
+  constexpr bool kCast = (K == kCastNearest || K == kCastAll);
+  constexpr bool kList = (K == kRayAll || K == kCastAll);
+  constexpr int QW = (K == kCastNearest || K == kCastAll) ? 4 * D : 2 * D;
+  using PL = PrimLayout<D, N>;
+  using NL = NodeLayout<D>;
+
+  // ---- load the query
+  RayPre<D> r;
+  float pmin[D], pmax[D];
+  const float* src = p.queries + size_t(q) * QW;
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    r.o[i] = src[i];
+    r.d[i] = src[D + i];
+    if constexpr (kCast) {
+      pmin[i] = src[2 * D + i];
+      pmax[i] = src[3 * D + i];
+    }
+  }
+  if constexpr (K != kOverlap) ray_prep<D>(r);
+  float limit = p.max_toi_arr ? p.max_toi_arr[q] : p.max_toi;
+
+  uint32_t best_leaf = kNoHit;
+  float best_t = 0.f;
+  float best_n[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) best_n[i] = 0.f;
+  uint32_t count = 0;
+  unsigned long long csr_base = 0;
+  if constexpr (K == kOverlap) {
+    if (p.fill) csr_base = p.csr_offsets[q];
+  }
+  uint32_t v_nodes = 0, v_nar = 0, v_hit = 0;
+
+  // ---- child box test
+  auto test_box = [&](const float* lo, const float* hi, float& te) -> bool {
+    if constexpr (K == kOverlap) {
+      te = 0.f;
+      return box_overlap<D>(lo, hi, r.o, r.d);  // region lo/hi were loaded into o/d
+    } else if constexpr (kCast) {
+      int ax;
+      return slab_grown<D>(r, lo, hi, pmin, pmax, limit, te, ax) && te <= limit;
+    } else {
+      int ax;
+      return slab<D>(r, lo, hi, limit, te, ax) && te <= limit;
+    }
+  };
+
+  // ---- root
+  if (STATS) v_nodes += 1;
+  float te_root, root_lo[D], root_hi[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    root_lo[i] = p.root_box[i];
+    root_hi[i] = p.root_box[D + i];
+  }
+  uint32_t code = p.root_code;
+  int sp = 0;
+  bool live = test_box(root_lo, root_hi, te_root);
+
+  while (live) {
+    if (!(code & kLeafBit)) {
+      // Interior: one child-pair record.
+      float rec[NL::vec * 4];
+      load_vec<NL::vec>(p.nodes + size_t(code) * NL::vec, rec);
+      const uint32_t ca = __float_as_uint(rec[4 * D]);
+      const uint32_t cb = __float_as_uint(rec[4 * D + 1]);
+      float ta, tb;
+      const bool pa = test_box(rec, rec + D, ta);
+      const bool pb = test_box(rec + 2 * D, rec + 3 * D, tb);
+      if (STATS) v_nodes += 2;
+      if (REF || !kNearest) {
+        // Reference order: child_a waits on the stack, child_b goes first.
+        if (pa) {
+          if (pb) {
+            s_code[sp][tid] = ca;
+            s_t[sp][tid] = ta;
+            ++sp;
+            code = cb;
+            continue;
+          }
+          code = ca;
+          continue;
+        }
+        if (pb) { code = cb; continue; }
+      } else {
+        if (pa && pb) {
+          const bool a_first = ta <= tb;
+          s_code[sp][tid] = a_first ? cb : ca;
+          s_t[sp][tid] = a_first ? tb : ta;
+          ++sp;
+          code = a_first ? ca : cb;
+          continue;
+        }
+        if (pa) { code = ca; continue; }
+        if (pb) { code = cb; continue; }
+      }
+    } else {
+      // Leaf: the primitives from its first position to the flagged last one.
+      uint32_t pos = code & ~kLeafBit;
+      for (;;) {
+        float rec[PL::vec * 4];
+        load_vec<PL::vec>(p.prims + size_t(pos) * PL::vec, rec);
+        const uint32_t idw = __float_as_uint(rec[PL::id_word]);
+        const uint32_t id = idw & ~kLeafBit;
+        if (accepts(p, id)) {
+          if constexpr (K == kOverlap) {
+            if (narrow_overlap<D, N>(rec, r.o, r.d)) {
+              if (p.fill) {
+                // ascending leaf order within the query's CSR segment
+                uint32_t j = count;
+                while (j > 0 && p.csr_leaves[csr_base + j - 1] > id) {
+                  p.csr_leaves[csr_base + j] = p.csr_leaves[csr_base + j - 1];
+                  --j;
+                }
+                p.csr_leaves[csr_base + j] = id;
+              }
+              ++count;
+            }
+          } else {
+            if (STATS) v_nar += 1;
+            float t, nrm[D];
+            if constexpr (K == kRayNearest) {
+              if (narrow_ray<D, N>(rec, r, limit, t, nrm)) {
+                if (STATS) v_hit += 1;
+                if (best_leaf == kNoHit || hit_before(t, id, best_t, best_leaf)) {
+                  best_leaf = id;
+                  best_t = t;
+                  limit = t;
+#pragma unroll
+                  for (int i = 0; i < D; ++i) best_n[i] = nrm[i];
+                }
+              }
+            } else if constexpr (K == kCastNearest) {
+              if (narrow_cast<D, N>(rec, r, pmin, pmax, limit, t, nrm)) {
+                if (best_leaf == kNoHit || hit_before(t, id, best_t, best_leaf)) {
+                  best_leaf = id;
+                  best_t = t;
+                  limit = t;
+#pragma unroll
+                  for (int i = 0; i < D; ++i) best_n[i] = nrm[i];
+                }
+              }
+            } else if constexpr (K == kRayAll) {
+              if constexpr (N == kNarrowSphere) {
+                if (p.crossings) {
+                  // Both roots of the unbounded ray (tests/crossings.rs:505-521).
+                  float oc[D];
+#pragma unroll
+                  for (int i = 0; i < D; ++i) oc[i] = fsub(r.o[i], rec[i]);
+                  float b = pdot<D>(oc, r.d);
+                  float disc = fsub(fmul(b, b), fsub(pdot<D>(oc, oc), fmul(rec[D], rec[D])));
+                  if (!(disc < 0.f)) {
+                    float sq = fsqrt(disc);
+                    float roots[2] = {fsub(-b, sq), fadd(-b, sq)};
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) {
+                      float tt = roots[j];
+                      if (tt >= 0.f && tt <= limit) {
+                        float pt[D];
+                        ray_at<D>(r.o, r.d, tt, pt);
+#pragma unroll
+                        for (int i = 0; i < D; ++i) nrm[i] = fsub(pt[i], rec[i]);
+                        normalize_or_zero<D>(nrm);
+                        if (STATS) v_hit += 1;
+                        list_insert<D>(p, q, count, tt, id, nrm);
+                      }
+                    }
+                  }
+                } else if (narrow_ray<D, N>(rec, r, limit, t, nrm)) {
+                  if (STATS) v_hit += 1;
+                  list_insert<D>(p, q, count, t, id, nrm);
+                }
+              } else {
+                if (narrow_ray<D, N>(rec, r, limit, t, nrm)) {
+                  if (STATS) v_hit += 1;
+                  list_insert<D>(p, q, count, t, id, nrm);
+                }
+              }
+            } else {  // kCastAll
+              if (narrow_cast<D, N>(rec, r, pmin, pmax, limit, t, nrm)) list_insert<D>(p, q, count, t, id, nrm);
+            }
+          }
+        }
+        if (idw & kLeafBit) break;
+        ++pos;
+      }
+    }
+    // Pop the next waiting child; drop it if its entry now lies beyond the
+    // shrunk limit (exactly the reference's slab verdict at pop time).
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      code = s_code[sp][tid];
+      const float t = s_t[sp][tid];
+      if (!kNearest || t <= limit) { found = true; break; }
+    }
+    if (!found) break;
+  }
+
+  // ---- write results
+  if constexpr (kNearest) {
+    p.out_leaf[q] = best_leaf;
+    if (p.out_toi) p.out_toi[q] = best_t;
+    if (p.out_sub) p.out_sub[q] = (best_leaf != kNoHit && p.sub) ? __ldg(p.sub + best_leaf) : kNoHit;
+    if (p.out_normal)
+#pragma unroll
+      for (int i = 0; i < D; ++i) p.out_normal[size_t(q) * D + i] = best_n[i];
+    if (p.out_point) {
+      float pt[D];
+      if (best_leaf != kNoHit) ray_at<D>(r.o, r.d, best_t, pt);
+      else
+#pragma unroll
+        for (int i = 0; i < D; ++i) pt[i] = 0.f;
+#pragma unroll
+      for (int i = 0; i < D; ++i) p.out_point[size_t(q) * D + i] = pt[i];
+    }
+  } else if constexpr (kList) {
+    // Entries past min(count, k) are left as they were.
+    p.out_count[q] = count;
+  } else {
+    if (!p.fill) p.out_count[q] = count;
+  }
+  if (STATS) {
+    c_vis += v_nodes;
+    c_nar += v_nar;
+    c_hit += v_hit;
+    if (p.query_stats) {
+      p.query_stats[size_t(q) * 4 + 0] = v_nodes;
+      p.query_stats[size_t(q) * 4 + 1] = v_nodes;
+      p.query_stats[size_t(q) * 4 + 2] = v_nar;
+      p.query_stats[size_t(q) * 4 + 3] = v_hit;
+    }
+  }
+}
+
+template <int D, int N, int K, bool REF, bool STATS>
+__global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
+  __shared__ uint32_t s_code[kStack][kThreads];
+  __shared__ float s_t[kStack][kThreads];
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  unsigned long long c_vis = 0, c_nar = 0, c_hit = 0;
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(p.counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= p.n) break;
+    const uint32_t q = base + lane;
+    if (q < p.n) run_query<D, N, K, REF, STATS>(p, q, tid, s_code, s_t, c_vis, c_nar, c_hit);
+  }
+  if (STATS) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      c_vis += __shfl_down_sync(0xffffffffu, c_vis, o);
+      c_nar += __shfl_down_sync(0xffffffffu, c_nar, o);
+      c_hit += __shfl_down_sync(0xffffffffu, c_hit, o);
+    }
+    if (lane == 0 && p.stats) {
+      atomicAdd(p.stats + 0, c_vis);
+      atomicAdd(p.stats + 1, c_vis);
+      atomicAdd(p.stats + 2, c_nar);
+      atomicAdd(p.stats + 3, c_hit);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Device refit: tree::refit (accel/tree.rs:54-75) over the fixed topology.
+//
+// One thread per leaf rewrites its primitives' records from the new leaf
+// parameters and unions their boxes into the leaf box, which it stores in the
+// parent's child slot. It then climbs: at each interior node an arrival
+// counter lets the second of the two children through, which unions the two
+// slots of that node's record into its own slot in its parent, and so on to
+// the root. Unions are min/max, exact in any order.
+// ---------------------------------------------------------------------------
+
+struct RefitLeaf {
+  uint32_t first;   // first position in the leaf-ordered primitive array
+  uint32_t count;
+  uint32_t parent;  // parent interior record << 1 | slot, or kNoHit for the root
+  uint32_t pad;
+};
+
+struct RefitParams {
+  float4* nodes;
+  float4* prims;
+  float* root_box;
+  const float* prim_data;  // new leaf parameters, indexed by leaf id
+  const uint32_t* prim_ids;
+  const RefitLeaf* leaves;
+  const uint32_t* parents;  // per interior record: parent << 1 | slot, or kNoHit
+  uint32_t* arrivals;       // per interior record, zeroed before the launch
+  uint32_t n_leaves;
+  uint32_t stride;          // floats per leaf parameter block
+};
+
+template <int D, int N>
+__device__ __forceinline__ void prim_box(const float* v, float* lo, float* hi) {
+  if constexpr (N == kNarrowAabb) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) { lo[i] = v[i]; hi[i] = v[D + i]; }
+  } else if constexpr (N == kNarrowSphere || N == kNarrowSphereNear) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) { lo[i] = fsub(v[i], v[D]); hi[i] = fadd(v[i], v[D]); }
+  } else {
+    tri_aabb(v, v + 3, v + 6, lo, hi);
+  }
+}
+
+template <int D>
+__device__ __forceinline__ void store_slot(const RefitParams& p, uint32_t parent, const float* lo, const float* hi) {
+  float* dst;
+  if (parent == kNoHit) {
+    dst = p.root_box;
+  } else {
+    dst = reinterpret_cast<float*>(p.nodes + size_t(parent >> 1) * NodeLayout<D>::vec) + (parent & 1u) * 2 * D;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    dst[i] = lo[i];
+    dst[D + i] = hi[i];
+  }
+}
+
+template <int D, int N> __global__ void __launch_bounds__(256) refit_kernel(const RefitParams p) {
+  const uint32_t li = blockIdx.x * blockDim.x + threadIdx.x;
+  if (li >= p.n_leaves) return;
+  const RefitLeaf L = p.leaves[li];
+  using PL = PrimLayout<D, N>;
+  float lo[D], hi[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) { lo[i] = __int_as_float(0x7f800000); hi[i] = __int_as_float(0xff800000); }
+  for (uint32_t j = 0; j < L.count; ++j) {
+    const uint32_t pos = L.first + j;
+    const uint32_t id = p.prim_ids[pos];
+    const float* v = p.prim_data + size_t(id) * p.stride;
+    float rec[PL::vec * 4];
+#pragma unroll
+    for (int w = 0; w < PL::vec * 4; ++w) rec[w] = 0.f;
+#pragma unroll
+    for (int w = 0; w < PL::payload; ++w) rec[w] = v[w];
+    rec[PL::id_word] = __uint_as_float(id | (j + 1 == L.count ? kLeafBit : 0u));
+    float4* dst = p.prims + size_t(pos) * PL::vec;
+#pragma unroll
+    for (int w = 0; w < PL::vec; ++w) dst[w] = make_float4(rec[4 * w], rec[4 * w + 1], rec[4 * w + 2], rec[4 * w + 3]);
+    float plo[D], phi[D];
+    prim_box<D, N>(rec, plo, phi);
+#pragma unroll
+    for (int i = 0; i < D; ++i) { lo[i] = fminf(lo[i], plo[i]); hi[i] = fmaxf(hi[i], phi[i]); }
+  }
+  uint32_t parent = L.parent;
+  store_slot<D>(p, parent, lo, hi);
+  while (parent != kNoHit) {
+    __threadfence();
+    const uint32_t node = parent >> 1;
+    if (atomicAdd(p.arrivals + node, 1u) == 0u) return;  // the sibling finishes this node
+    __threadfence();
+    const float* rec = reinterpret_cast<const float*>(p.nodes + size_t(node) * NodeLayout<D>::vec);
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      lo[i] = fminf(__ldcg(rec + i), __ldcg(rec + 2 * D + i));
+      hi[i] = fmaxf(__ldcg(rec + D + i), __ldcg(rec + 3 * D + i));
+    }
+    parent = p.parents[node];
+    store_slot<D>(p, parent, lo, hi);
+  }
+}
+
+// Function-pointer table entry for one (D, narrow) pair.
+struct KernelSet {
+  const void* ray_nearest[2][2];  // [ref][stats]
+  const void* ray_all[2];         // [stats]
+  const void* cast_nearest[2];    // [ref]
+  const void* cast_all;
+  const void* overlap;
+  const void* refit_leaves;
+};
+
+template <int D, int N> KernelSet make_kernel_set() {
+  KernelSet s;
+  s.ray_nearest[0][0] = (const void*)query_kernel<D, N, kRayNearest, false, false>;
+  s.ray_nearest[0][1] = (const void*)query_kernel<D, N, kRayNearest, false, true>;
+  s.ray_nearest[1][0] = (const void*)query_kernel<D, N, kRayNearest, true, false>;
+  s.ray_nearest[1][1] = (const void*)query_kernel<D, N, kRayNearest, true, true>;
+  s.ray_all[0] = (const void*)query_kernel<D, N, kRayAll, true, false>;
+  s.ray_all[1] = (const void*)query_kernel<D, N, kRayAll, true, true>;
+  s.cast_nearest[0] = (const void*)query_kernel<D, N, kCastNearest, false, false>;
+  s.cast_nearest[1] = (const void*)query_kernel<D, N, kCastNearest, true, false>;
+  s.cast_all = (const void*)query_kernel<D, N, kCastAll, true, false>;
+  s.overlap = (const void*)query_kernel<D, N, kOverlap, true, false>;
+  s.refit_leaves = (const void*)refit_kernel<D, N>;
+  return s;
+}
+
+}  // namespace sq

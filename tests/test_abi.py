@@ -1,0 +1,70 @@
+"""The C ABI library loads, exports every symbol include/sq.h declares, and
+behaves on a machine without a GPU (no compute call is made here)."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import spatial_query_b200 as sq
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "sq.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(sq_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_query_surface():
+    syms = declared_symbols()
+    for name in ["sq_ctx_create", "sq_bvh_upload", "sq_bvh_refit", "sq_raycast_nearest", "sq_raycast_all",
+                 "sq_raycast_crossings", "sq_shapecast_nearest", "sq_shapecast_all", "sq_overlap", "sq_tree_build"]:
+        assert name in syms
+
+
+def test_library_exports_every_declared_symbol():
+    lib = sq.lib()
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+    assert set(declared_symbols()) <= set(sq.SIGNATURES)
+
+
+def test_version():
+    assert sq.lib().sq_version() == 1
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-device path")
+def test_headless_returns_none_without_a_device():
+    """GpuRaycaster::headless returns None with no adapter (gpu/mod.rs:308-324)."""
+    g = sq.Geometry("balls", 3, np.array([[0, 0, 0, 1]], np.float32))
+    assert sq.GpuRaycaster.headless(sq.HostBvh.build(g), g) is None
+
+
+def test_prim_aabbs_match_provider_bounds():
+    tri = np.array([[0, 0, 0, 1, 2, -1, -3, 0.5, 4]], np.float32)
+    a = sq.Geometry("tris", 3, tri).world_aabbs()
+    assert np.array_equal(a, np.array([[-3, 0, -1, 1, 2, 4]], np.float32))
+    b = sq.Geometry("balls", 2, np.array([[1, 2, 0.5]], np.float32)).world_aabbs()
+    assert np.array_equal(b, np.array([[0.5, 1.5, 1.5, 2.5]], np.float32))
+
+
+def test_tree_build_rejects_small_capacity():
+    lib = sq.lib()
+    import ctypes as C
+    a = np.zeros((10, 6), np.float32)
+    nn = C.c_uint32(0)
+    out = np.empty((4, 6), np.float32)
+    small = np.empty(4, np.uint32)
+    rc = lib.sq_tree_build(3, 10, a.ctypes.data, 1, 4, C.byref(nn), out.ctypes.data, small.ctypes.data,
+                           small.ctypes.data, small.ctypes.data, np.empty(10, np.uint32).ctypes.data)
+    assert rc == sq.SQ_ERR_CAPACITY
