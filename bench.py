@@ -221,8 +221,9 @@ def main():
     geom = sq.Geometry("tris", 3, s["prims"])
     tree = sq.HostBvh.build(geom)
     ctx = sq.Context(local)
-    stream = torch.cuda.current_stream()
-    ctx.set_stream(stream.cuda_stream)
+    # Every kernel, flush and event goes on the context's own stream.
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    torch.cuda.set_stream(stream)
     ctx.set_order(sq.ORDER_REFERENCE if args.order == "reference" else sq.ORDER_NEAR_FIRST)
     scene = sq.DeviceBvh(ctx, tree, geom)
     info = scene.info()

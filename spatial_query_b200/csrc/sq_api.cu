@@ -12,6 +12,7 @@
 #include <cuda/std/functional>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -56,7 +57,7 @@ struct sq_ctx {
   unsigned long long* d_stats = nullptr;
   DevBuf arena;
   uint64_t launches = 0;
-  std::unordered_map<const void*, int> occ;
+  std::unordered_map<uint64_t, int> occ;  // (kernel, dynamic smem) -> resident blocks per SM
 };
 
 struct sq_bvh {
@@ -76,6 +77,7 @@ struct sq_bvh {
   uint32_t* d_parents = nullptr;
   uint32_t* d_arrivals = nullptr;
   float* d_refit_in = nullptr;  // staging for host refit data
+  int* d_nonfinite = nullptr;   // non-zero when some node bound is not finite
   KernelSet ks{};
   size_t bytes = 0;
   std::vector<uint32_t> h_iidx;  // host node -> interior record (or kNoHit)
@@ -150,24 +152,31 @@ struct Carve {
   }
 };
 
-int occupancy(sq_ctx* ctx, const void* fn) {
-  auto it = ctx->occ.find(fn);
+int occupancy(sq_ctx* ctx, const void* fn, size_t smem) {
+  const uint64_t key = uint64_t(uintptr_t(fn)) * 131 + smem;
+  auto it = ctx->occ.find(key);
   if (it != ctx->occ.end()) return it->second;
   int nb = 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kThreads, 0) != cudaSuccess || nb < 1) nb = 1;
-  ctx->occ[fn] = nb;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kThreads, smem) != cudaSuccess || nb < 1) nb = 1;
+  ctx->occ[key] = nb;
   return nb;
 }
 
-int32_t launch_persistent(sq_ctx* ctx, const void* fn, QueryParams& p) {
+// The persistent grid: (resident blocks per SM) x (SM count), no more blocks
+// than the queries need. The traversal stack is dynamic shared memory sized
+// to the tree depth, so shallow trees leave room for more resident warps.
+int32_t launch_persistent(sq_ctx* ctx, const void* fn, QueryParams& p, uint32_t depth) {
   uint32_t* ctr = ctx->d_counters + (ctx->slot++ % kCounterSlots);
   CK(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), ctx->stream));
   p.counter = ctr;
-  int bps = ctx->blocks_per_sm > 0 ? ctx->blocks_per_sm : occupancy(ctx, fn);
+  p.stack = int(std::max<uint32_t>(depth, 1));
+  const size_t smem = size_t(p.stack) * kThreads * 8;
+  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  int bps = ctx->blocks_per_sm > 0 ? ctx->blocks_per_sm : occupancy(ctx, fn, smem);
   uint64_t want = (uint64_t(p.n) + kThreads - 1) / kThreads;
   uint64_t grid = std::min<uint64_t>(uint64_t(ctx->sm_count) * bps, std::max<uint64_t>(want, 1));
   void* args[] = {&p};
-  CK(cudaLaunchKernel(fn, dim3(unsigned(grid)), dim3(kThreads), args, 0, ctx->stream));
+  CK(cudaLaunchKernel(fn, dim3(unsigned(grid)), dim3(kThreads), args, smem, ctx->stream));
   ctx->launches++;
   return SQ_OK;
 }
@@ -179,6 +188,7 @@ void base_params(const sq_bvh* b, const sq_filter* f, QueryParams& p) {
   p.layers = b->d_layers;
   p.sub = b->d_sub;
   p.root_box = b->d_root;
+  p.nonfinite = b->d_nonfinite;
   p.root_code = b->root_code;
   p.mask = f ? f->layer_mask : ~0ull;
   p.exclude = f ? f->exclude : -1;
@@ -227,7 +237,7 @@ int32_t nearest_core(sq_ctx* ctx, const sq_bvh* b, bool cast, const float* d_q, 
     fn = b->ks.ray_nearest[ref][stats ? 1 : 0];
     if (stats) p.stats = ctx->d_stats;
   }
-  return launch_persistent(ctx, fn, p);
+  return launch_persistent(ctx, fn, p, b->depth);
 }
 
 int32_t list_core(sq_ctx* ctx, const sq_bvh* b, int kind, const float* d_q, uint32_t n, float max_toi,
@@ -258,7 +268,7 @@ int32_t list_core(sq_ctx* ctx, const sq_bvh* b, int kind, const float* d_q, uint
     fn = b->ks.ray_all[stats ? 1 : 0];
     if (stats) p.stats = ctx->d_stats;
   }
-  return launch_persistent(ctx, fn, p);
+  return launch_persistent(ctx, fn, p, b->depth);
 }
 
 int32_t stats_begin(sq_ctx* ctx, sq_query_stats* st) {
@@ -413,7 +423,8 @@ extern "C" int32_t sq_bvh_upload(sq_ctx* ctx, int32_t dim, int32_t narrow, uint3
     }
   }
   b->depth = depth[0];
-  if (b->depth > uint32_t(kStack)) return fail(ctx, SQ_ERR_DEPTH, "tree depth " + std::to_string(b->depth) + " exceeds the traversal stack");
+  if (b->depth > uint32_t(kMaxStack))
+    return fail(ctx, SQ_ERR_DEPTH, "tree depth " + std::to_string(b->depth) + " exceeds the traversal stack");
   // The leaves must partition the index array and the index array must be a
   // permutation: every kernel walk of a leaf then ends on its own last
   // primitive, inside the array.
@@ -506,6 +517,10 @@ extern "C" int32_t sq_bvh_upload(sq_ctx* ctx, int32_t dim, int32_t narrow, uint3
   if ((rc = up((void**)&b->d_arrivals, nullptr, parents.size() * 4))) return cleanup(rc);
   if (layers && (rc = up((void**)&b->d_layers, layers, size_t(n_prims) * 8))) return cleanup(rc);
   if (sub_objects && (rc = up((void**)&b->d_sub, sub_objects, size_t(n_prims) * 4))) return cleanup(rc);
+  int nonfinite = 0;
+  for (size_t k = 0; k < size_t(n_nodes) * 2 * D; ++k)
+    if (!std::isfinite(node_bounds[k])) nonfinite = 1;
+  if ((rc = up((void**)&b->d_nonfinite, &nonfinite, sizeof(int)))) return cleanup(rc);
   *out = b.release();
   return SQ_OK;
 }
@@ -514,7 +529,7 @@ extern "C" int32_t sq_bvh_destroy(sq_bvh* b) {
   if (!b) return SQ_OK;
   cudaSetDevice(b->device);
   void* ptrs[] = {b->d_nodes, b->d_prims, b->d_root, b->d_layers, b->d_sub, b->d_prim_ids,
-                  b->d_leaves, b->d_parents, b->d_arrivals, b->d_refit_in};
+                  b->d_leaves, b->d_parents, b->d_arrivals, b->d_refit_in, b->d_nonfinite};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete b;
@@ -541,7 +556,9 @@ extern "C" int32_t sq_bvh_refit_d(sq_ctx* ctx, sq_bvh* b, const float* d_prim_da
   if (b->n_nodes == 0) return SQ_OK;
   if (!d_prim_data) return fail(ctx, SQ_ERR_INVALID, "null prim data");
   CK(cudaMemsetAsync(b->d_arrivals, 0, size_t(std::max<uint32_t>(b->n_interior, 1)) * 4, ctx->stream));
+  CK(cudaMemsetAsync(b->d_nonfinite, 0, sizeof(int), ctx->stream));
   RefitParams p;
+  p.nonfinite = b->d_nonfinite;
   p.nodes = b->d_nodes;
   p.prims = b->d_prims;
   p.root_box = b->d_root;
@@ -676,7 +693,7 @@ int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint3
     p.n = n;
     p.out_count = d_counts;
     p.fill = 0;
-    int32_t rc = launch_persistent(ctx, b->ks.overlap, p);
+    int32_t rc = launch_persistent(ctx, b->ks.overlap, p, b->depth);
     if (rc) return rc;
   }
   CK(cub::DeviceScan::ExclusiveScan(temp, temp_bytes, d_counts, (unsigned long long*)d_offsets, cuda::std::plus<>{},
@@ -696,7 +713,7 @@ int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint3
     p.fill = 1;
     p.csr_offsets = (const unsigned long long*)d_offsets;
     p.csr_leaves = d_leaves;
-    int32_t rc = launch_persistent(ctx, b->ks.overlap, p);
+    int32_t rc = launch_persistent(ctx, b->ks.overlap, p, b->depth);
     if (rc) return rc;
   }
   return SQ_OK;

@@ -83,6 +83,28 @@ __device__ __forceinline__ bool slab(const RayPre<D>& r, const float* lo, const 
   return ok && !(tmin > tmax);
 }
 
+// The slab for a finite ray against a finite box. With no NaN possible, the
+// compare-and-swap of the reference equals a min/max pair and its
+// `if t > t_min` update equals a max, except that a max may return -0 where
+// the reference keeps +0: only the returned entry can show that sign, so it is
+// normalised with + 0. Callers use this form only for rays with no parallel
+// axis and finite origin, direction, probe and limit, against a scene whose
+// bounds are all finite; other rays take `slab`.
+template <int D>
+__device__ __forceinline__ bool slab_fast(const RayPre<D>& r, const float* lo, const float* hi, float max_toi,
+                                          float& t_enter) {
+  float tmin = 0.f, tmax = max_toi;
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    const float t1 = fmul(fsub(lo[i], r.o[i]), r.inv[i]);
+    const float t2 = fmul(fsub(hi[i], r.o[i]), r.inv[i]);
+    tmin = fmaxf(tmin, fminf(t1, t2));
+    tmax = fminf(tmax, fmaxf(t1, t2));
+  }
+  t_enter = fadd(tmin, 0.0f);
+  return !(tmin > tmax);
+}
+
 // The same slab against a box grown by a probe: ShapeCast::broadphase
 // (query/shapecast.rs:70-73): grown = [lo - probe.max, hi - probe.min].
 template <int D>
@@ -95,6 +117,19 @@ __device__ __forceinline__ bool slab_grown(const RayPre<D>& r, const float* lo, 
     ghi[i] = fsub(hi[i], pmin[i]);
   }
   return slab<D>(r, glo, ghi, max_toi, t_enter, axis);
+}
+
+template <int D>
+__device__ __forceinline__ bool slab_grown_fast(const RayPre<D>& r, const float* lo, const float* hi,
+                                                const float* pmin, const float* pmax, float max_toi,
+                                                float& t_enter) {
+  float glo[D], ghi[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    glo[i] = fsub(lo[i], pmax[i]);
+    ghi[i] = fsub(hi[i], pmin[i]);
+  }
+  return slab_fast<D>(r, glo, ghi, max_toi, t_enter);
 }
 
 // Aabb::intersects (aabb.rs:101-108): touching faces count.

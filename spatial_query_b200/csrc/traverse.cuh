@@ -28,7 +28,7 @@ enum Narrow : int { kNarrowAabb = 0, kNarrowSphere = 1, kNarrowSphereNear = 2, k
 enum QKind : int { kRayNearest = 0, kRayAll = 1, kCastNearest = 2, kCastAll = 3, kOverlap = 4 };
 
 constexpr int kThreads = 128;
-constexpr int kStack = 32;
+constexpr int kMaxStack = 96;  // deepest tree accepted (96 KB of stack per block)
 
 template <int D> struct NodeLayout {
   static constexpr int words = 4 * D + 2;  // a.lo a.hi b.lo b.hi code_a code_b
@@ -66,7 +66,9 @@ struct QueryParams {
   unsigned long long mask;
   long long exclude;
   const float* root_box;  // min[D], max[D] of the root (device memory: refit updates it)
+  const int* nonfinite;   // non-zero when some node bound is not finite (device memory)
   float max_toi;
+  int stack;              // traversal-stack entries per thread (dynamic shared memory)
   uint32_t root_code;
   uint32_t n;
   uint32_t k;
@@ -185,268 +187,320 @@ __device__ __forceinline__ void list_insert(const QueryParams& p, uint32_t q, ui
     for (int i = 0; i < D; ++i) p.out_normal[(base + j) * D + i] = n[i];
 }
 
+// Per-lane traversal state of one query.
+template <int D, int K> struct Lane {
+  RayPre<D> r;
+  float pmin[D], pmax[D];
+  float limit;
+  uint32_t q;
+  uint32_t code;
+  int sp;
+  bool fast;
+  uint32_t best_leaf;
+  float best_t;
+  float best_n[D];
+  uint32_t count;
+  unsigned long long csr_base;
+  uint32_t v_nodes, v_nar, v_hit;
+};
+
+// The persistent query kernel. Each warp keeps 32 queries in flight; a lane
+// whose query finishes takes the next one from the shared counter at the top
+// of the loop (one atomic per warp per refill), so a warp never idles on its
+// slowest query. Between refills a lane descends interior records until it
+// reaches a leaf, tests that leaf's primitives and pops the next waiting
+// child (Aila and Laine's while-while loop with dynamic fetch).
 template <int D, int N, int K, bool REF, bool STATS>
-__device__ __forceinline__ void run_query(const QueryParams& p, uint32_t q, int tid, uint32_t (*s_code)[kThreads],
-                                          float (*s_t)[kThreads], unsigned long long& c_vis,
-                                          unsigned long long& c_nar, unsigned long long& c_hit) {
+__global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   constexpr bool kNearest = (K == kRayNearest || K == kCastNearest);
   constexpr bool kCast = (K == kCastNearest || K == kCastAll);
   constexpr bool kList = (K == kRayAll || K == kCastAll);
-  constexpr int QW = (K == kCastNearest || K == kCastAll) ? 4 * D : 2 * D;
+  constexpr int QW = kCast ? 4 * D : 2 * D;
   using PL = PrimLayout<D, N>;
   using NL = NodeLayout<D>;
+  constexpr uint32_t FULL = 0xffffffffu;
 
-  // ---- load the query
-  RayPre<D> r;
-  float pmin[D], pmax[D];
-  const float* src = p.queries + size_t(q) * QW;
-#pragma unroll
-  for (int i = 0; i < D; ++i) {
-    r.o[i] = src[i];
-    r.d[i] = src[D + i];
-    if constexpr (kCast) {
-      pmin[i] = src[2 * D + i];
-      pmax[i] = src[3 * D + i];
-    }
-  }
-  if constexpr (K != kOverlap) ray_prep<D>(r);
-  float limit = p.max_toi_arr ? p.max_toi_arr[q] : p.max_toi;
+  extern __shared__ uint32_t smem[];
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int S = p.stack;
+  uint32_t* s_code = smem;
+  float* s_t = reinterpret_cast<float*>(smem + S * kThreads);
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  const bool scene_finite = p.nonfinite ? (*p.nonfinite == 0) : true;
 
-  uint32_t best_leaf = kNoHit;
-  float best_t = 0.f;
-  float best_n[D];
-#pragma unroll
-  for (int i = 0; i < D; ++i) best_n[i] = 0.f;
-  uint32_t count = 0;
-  unsigned long long csr_base = 0;
-  if constexpr (K == kOverlap) {
-    if (p.fill) csr_base = p.csr_offsets[q];
-  }
-  uint32_t v_nodes = 0, v_nar = 0, v_hit = 0;
+  unsigned long long c_vis = 0, c_nar = 0, c_hit = 0;
+  Lane<D, K> L;
+  bool live = false, exhausted = false;
 
-  // ---- child box test
+  // Box test of one child (or the root) against the lane's query.
   auto test_box = [&](const float* lo, const float* hi, float& te) -> bool {
     if constexpr (K == kOverlap) {
       te = 0.f;
-      return box_overlap<D>(lo, hi, r.o, r.d);  // region lo/hi were loaded into o/d
+      return box_overlap<D>(lo, hi, L.r.o, L.r.d);  // region lo / hi sit in o / d
     } else if constexpr (kCast) {
+      if (L.fast) return slab_grown_fast<D>(L.r, lo, hi, L.pmin, L.pmax, L.limit, te);
       int ax;
-      return slab_grown<D>(r, lo, hi, pmin, pmax, limit, te, ax) && te <= limit;
+      return slab_grown<D>(L.r, lo, hi, L.pmin, L.pmax, L.limit, te, ax) && te <= L.limit;
     } else {
+      if (L.fast) return slab_fast<D>(L.r, lo, hi, L.limit, te);
       int ax;
-      return slab<D>(r, lo, hi, limit, te, ax) && te <= limit;
+      return slab<D>(L.r, lo, hi, L.limit, te, ax) && te <= L.limit;
     }
   };
 
-  // ---- root
-  if (STATS) v_nodes += 1;
-  float te_root, root_lo[D], root_hi[D];
-#pragma unroll
-  for (int i = 0; i < D; ++i) {
-    root_lo[i] = p.root_box[i];
-    root_hi[i] = p.root_box[D + i];
-  }
-  uint32_t code = p.root_code;
-  int sp = 0;
-  bool live = test_box(root_lo, root_hi, te_root);
+  // Pops the next waiting child whose entry still lies within the limit
+  // (exactly the reference's slab verdict at pop time). False: stack empty.
+  auto pop = [&]() -> bool {
+    while (L.sp > 0) {
+      --L.sp;
+      L.code = s_code[L.sp * kThreads + tid];
+      const float t = s_t[L.sp * kThreads + tid];
+      if (!kNearest || t <= L.limit) return true;
+    }
+    return false;
+  };
 
-  while (live) {
-    if (!(code & kLeafBit)) {
-      // Interior: one child-pair record.
-      float rec[NL::vec * 4];
-      load_vec<NL::vec>(p.nodes + size_t(code) * NL::vec, rec);
-      const uint32_t ca = __float_as_uint(rec[4 * D]);
-      const uint32_t cb = __float_as_uint(rec[4 * D + 1]);
-      float ta, tb;
-      const bool pa = test_box(rec, rec + D, ta);
-      const bool pb = test_box(rec + 2 * D, rec + 3 * D, tb);
-      if (STATS) v_nodes += 2;
-      if (REF || !kNearest) {
-        // Reference order: child_a waits on the stack, child_b goes first.
-        if (pa) {
-          if (pb) {
-            s_code[sp][tid] = ca;
-            s_t[sp][tid] = ta;
-            ++sp;
-            code = cb;
-            continue;
-          }
-          code = ca;
-          continue;
-        }
-        if (pb) { code = cb; continue; }
-      } else {
-        if (pa && pb) {
-          const bool a_first = ta <= tb;
-          s_code[sp][tid] = a_first ? cb : ca;
-          s_t[sp][tid] = a_first ? tb : ta;
-          ++sp;
-          code = a_first ? ca : cb;
-          continue;
-        }
-        if (pa) { code = ca; continue; }
-        if (pb) { code = cb; continue; }
+  auto finish = [&]() {
+    const uint32_t q = L.q;
+    if constexpr (kNearest) {
+      p.out_leaf[q] = L.best_leaf;
+      if (p.out_toi) p.out_toi[q] = L.best_t;
+      if (p.out_sub) p.out_sub[q] = (L.best_leaf != kNoHit && p.sub) ? __ldg(p.sub + L.best_leaf) : kNoHit;
+      if (p.out_normal) {
+#pragma unroll
+        for (int i = 0; i < D; ++i) p.out_normal[size_t(q) * D + i] = L.best_n[i];
       }
+      if (p.out_point) {
+        float pt[D];
+        if (L.best_leaf != kNoHit) {
+          ray_at<D>(L.r.o, L.r.d, L.best_t, pt);
+        } else {
+#pragma unroll
+          for (int i = 0; i < D; ++i) pt[i] = 0.f;
+        }
+#pragma unroll
+        for (int i = 0; i < D; ++i) p.out_point[size_t(q) * D + i] = pt[i];
+      }
+    } else if constexpr (kList) {
+      p.out_count[q] = L.count;  // entries past min(count, k) are left as they were
     } else {
-      // Leaf: the primitives from its first position to the flagged last one.
-      uint32_t pos = code & ~kLeafBit;
-      for (;;) {
-        float rec[PL::vec * 4];
-        load_vec<PL::vec>(p.prims + size_t(pos) * PL::vec, rec);
-        const uint32_t idw = __float_as_uint(rec[PL::id_word]);
-        const uint32_t id = idw & ~kLeafBit;
-        if (accepts(p, id)) {
-          if constexpr (K == kOverlap) {
-            if (narrow_overlap<D, N>(rec, r.o, r.d)) {
-              if (p.fill) {
-                // ascending leaf order within the query's CSR segment
-                uint32_t j = count;
-                while (j > 0 && p.csr_leaves[csr_base + j - 1] > id) {
-                  p.csr_leaves[csr_base + j] = p.csr_leaves[csr_base + j - 1];
-                  --j;
-                }
-                p.csr_leaves[csr_base + j] = id;
+      if (!p.fill) p.out_count[q] = L.count;
+    }
+    if (STATS) {
+      c_vis += L.v_nodes;
+      c_nar += L.v_nar;
+      c_hit += L.v_hit;
+      if (p.query_stats) {
+        p.query_stats[size_t(q) * 4 + 0] = L.v_nodes;
+        p.query_stats[size_t(q) * 4 + 1] = L.v_nodes;
+        p.query_stats[size_t(q) * 4 + 2] = L.v_nar;
+        p.query_stats[size_t(q) * 4 + 3] = L.v_hit;
+      }
+    }
+  };
+
+  // Loads query q and tests the root. False when the query is already done.
+  auto start = [&](uint32_t q) -> bool {
+    L.q = q;
+    const float* src = p.queries + size_t(q) * QW;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      L.r.o[i] = src[i];
+      L.r.d[i] = src[D + i];
+      if constexpr (kCast) {
+        L.pmin[i] = src[2 * D + i];
+        L.pmax[i] = src[3 * D + i];
+      }
+    }
+    L.limit = p.max_toi_arr ? p.max_toi_arr[q] : p.max_toi;
+    if constexpr (K != kOverlap) {
+      ray_prep<D>(L.r);
+      bool f = scene_finite && L.r.par == 0u && !isnan(L.limit);
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        f = f && isfinite(L.r.o[i]) && isfinite(L.r.d[i]);
+        if constexpr (kCast) f = f && isfinite(L.pmin[i]) && isfinite(L.pmax[i]);
+      }
+      L.fast = f;
+    } else {
+      L.fast = false;
+    }
+    L.best_leaf = kNoHit;
+    L.best_t = 0.f;
+#pragma unroll
+    for (int i = 0; i < D; ++i) L.best_n[i] = 0.f;
+    L.count = 0;
+    L.csr_base = 0;
+    if constexpr (K == kOverlap) {
+      if (p.fill) L.csr_base = p.csr_offsets[q];
+    }
+    L.v_nodes = STATS ? 1u : 0u;
+    L.v_nar = 0;
+    L.v_hit = 0;
+    L.sp = 0;
+    L.code = p.root_code;
+    float lo[D], hi[D], te;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      lo[i] = p.root_box[i];
+      hi[i] = p.root_box[D + i];
+    }
+    return test_box(lo, hi, te);
+  };
+
+  // Tests the primitives of the leaf in L.code.
+  auto leaf = [&]() {
+    uint32_t pos = L.code & ~kLeafBit;
+    for (;;) {
+      float rec[PL::vec * 4];
+      load_vec<PL::vec>(p.prims + size_t(pos) * PL::vec, rec);
+      const uint32_t idw = __float_as_uint(rec[PL::id_word]);
+      const uint32_t id = idw & ~kLeafBit;
+      if (accepts(p, id)) {
+        if constexpr (K == kOverlap) {
+          if (narrow_overlap<D, N>(rec, L.r.o, L.r.d)) {
+            if (p.fill) {
+              // ascending leaf order within the query's CSR segment
+              uint32_t j = L.count;
+              while (j > 0 && p.csr_leaves[L.csr_base + j - 1] > id) {
+                p.csr_leaves[L.csr_base + j] = p.csr_leaves[L.csr_base + j - 1];
+                --j;
               }
-              ++count;
+              p.csr_leaves[L.csr_base + j] = id;
             }
-          } else {
-            if (STATS) v_nar += 1;
-            float t, nrm[D];
-            if constexpr (K == kRayNearest) {
-              if (narrow_ray<D, N>(rec, r, limit, t, nrm)) {
-                if (STATS) v_hit += 1;
-                if (best_leaf == kNoHit || hit_before(t, id, best_t, best_leaf)) {
-                  best_leaf = id;
-                  best_t = t;
-                  limit = t;
+            ++L.count;
+          }
+        } else {
+          if (STATS) L.v_nar += 1;
+          float t, nrm[D];
+          if constexpr (K == kRayNearest || K == kCastNearest) {
+            bool h;
+            if constexpr (K == kRayNearest) h = narrow_ray<D, N>(rec, L.r, L.limit, t, nrm);
+            else h = narrow_cast<D, N>(rec, L.r, L.pmin, L.pmax, L.limit, t, nrm);
+            if (h) {
+              if (STATS) L.v_hit += 1;
+              if (L.best_leaf == kNoHit || hit_before(t, id, L.best_t, L.best_leaf)) {
+                L.best_leaf = id;
+                L.best_t = t;
+                L.limit = t;
 #pragma unroll
-                  for (int i = 0; i < D; ++i) best_n[i] = nrm[i];
-                }
+                for (int i = 0; i < D; ++i) L.best_n[i] = nrm[i];
               }
-            } else if constexpr (K == kCastNearest) {
-              if (narrow_cast<D, N>(rec, r, pmin, pmax, limit, t, nrm)) {
-                if (best_leaf == kNoHit || hit_before(t, id, best_t, best_leaf)) {
-                  best_leaf = id;
-                  best_t = t;
-                  limit = t;
+            }
+          } else if constexpr (K == kRayAll) {
+            if constexpr (N == kNarrowSphere) {
+              if (p.crossings) {
+                // Both roots of the unbounded ray (tests/crossings.rs:505-521).
+                float oc[D];
 #pragma unroll
-                  for (int i = 0; i < D; ++i) best_n[i] = nrm[i];
-                }
-              }
-            } else if constexpr (K == kRayAll) {
-              if constexpr (N == kNarrowSphere) {
-                if (p.crossings) {
-                  // Both roots of the unbounded ray (tests/crossings.rs:505-521).
-                  float oc[D];
+                for (int i = 0; i < D; ++i) oc[i] = fsub(L.r.o[i], rec[i]);
+                const float b = pdot<D>(oc, L.r.d);
+                const float disc = fsub(fmul(b, b), fsub(pdot<D>(oc, oc), fmul(rec[D], rec[D])));
+                if (!(disc < 0.f)) {
+                  const float sq = fsqrt(disc);
+                  const float roots[2] = {fsub(-b, sq), fadd(-b, sq)};
 #pragma unroll
-                  for (int i = 0; i < D; ++i) oc[i] = fsub(r.o[i], rec[i]);
-                  float b = pdot<D>(oc, r.d);
-                  float disc = fsub(fmul(b, b), fsub(pdot<D>(oc, oc), fmul(rec[D], rec[D])));
-                  if (!(disc < 0.f)) {
-                    float sq = fsqrt(disc);
-                    float roots[2] = {fsub(-b, sq), fadd(-b, sq)};
+                  for (int j = 0; j < 2; ++j) {
+                    const float tt = roots[j];
+                    if (tt >= 0.f && tt <= L.limit) {
+                      float pt[D];
+                      ray_at<D>(L.r.o, L.r.d, tt, pt);
 #pragma unroll
-                    for (int j = 0; j < 2; ++j) {
-                      float tt = roots[j];
-                      if (tt >= 0.f && tt <= limit) {
-                        float pt[D];
-                        ray_at<D>(r.o, r.d, tt, pt);
-#pragma unroll
-                        for (int i = 0; i < D; ++i) nrm[i] = fsub(pt[i], rec[i]);
-                        normalize_or_zero<D>(nrm);
-                        if (STATS) v_hit += 1;
-                        list_insert<D>(p, q, count, tt, id, nrm);
-                      }
+                      for (int i = 0; i < D; ++i) nrm[i] = fsub(pt[i], rec[i]);
+                      normalize_or_zero<D>(nrm);
+                      if (STATS) L.v_hit += 1;
+                      list_insert<D>(p, L.q, L.count, tt, id, nrm);
                     }
                   }
-                } else if (narrow_ray<D, N>(rec, r, limit, t, nrm)) {
-                  if (STATS) v_hit += 1;
-                  list_insert<D>(p, q, count, t, id, nrm);
                 }
-              } else {
-                if (narrow_ray<D, N>(rec, r, limit, t, nrm)) {
-                  if (STATS) v_hit += 1;
-                  list_insert<D>(p, q, count, t, id, nrm);
-                }
+              } else if (narrow_ray<D, N>(rec, L.r, L.limit, t, nrm)) {
+                if (STATS) L.v_hit += 1;
+                list_insert<D>(p, L.q, L.count, t, id, nrm);
               }
-            } else {  // kCastAll
-              if (narrow_cast<D, N>(rec, r, pmin, pmax, limit, t, nrm)) list_insert<D>(p, q, count, t, id, nrm);
+            } else if (narrow_ray<D, N>(rec, L.r, L.limit, t, nrm)) {
+              if (STATS) L.v_hit += 1;
+              list_insert<D>(p, L.q, L.count, t, id, nrm);
             }
+          } else {  // kCastAll
+            if (narrow_cast<D, N>(rec, L.r, L.pmin, L.pmax, L.limit, t, nrm)) list_insert<D>(p, L.q, L.count, t, id, nrm);
           }
         }
-        if (idw & kLeafBit) break;
-        ++pos;
+      }
+      if (idw & kLeafBit) break;
+      ++pos;
+    }
+  };
+
+  for (;;) {
+    // Refill the lanes without a query.
+    const bool need = !live && !exhausted;
+    const uint32_t need_mask = __ballot_sync(FULL, need);
+    if (need_mask) {
+      const int leader = __ffs(need_mask) - 1;
+      uint32_t base = 0;
+      if (lane == leader) base = atomicAdd(p.counter, uint32_t(__popc(need_mask)));
+      base = __shfl_sync(FULL, base, leader);
+      if (need) {
+        const uint32_t q = base + uint32_t(__popc(need_mask & lt_mask));
+        if (q < p.n) {
+          live = start(q);
+          if (!live) finish();
+        } else {
+          exhausted = true;
+        }
       }
     }
-    // Pop the next waiting child; drop it if its entry now lies beyond the
-    // shrunk limit (exactly the reference's slab verdict at pop time).
-    bool found = false;
-    while (sp > 0) {
-      --sp;
-      code = s_code[sp][tid];
-      const float t = s_t[sp][tid];
-      if (!kNearest || t <= limit) { found = true; break; }
+    const uint32_t live_mask = __ballot_sync(FULL, live);
+    if (!live_mask) {
+      if (__all_sync(FULL, exhausted)) break;
+      continue;
     }
-    if (!found) break;
-  }
-
-  // ---- write results
-  if constexpr (kNearest) {
-    p.out_leaf[q] = best_leaf;
-    if (p.out_toi) p.out_toi[q] = best_t;
-    if (p.out_sub) p.out_sub[q] = (best_leaf != kNoHit && p.sub) ? __ldg(p.sub + best_leaf) : kNoHit;
-    if (p.out_normal)
-#pragma unroll
-      for (int i = 0; i < D; ++i) p.out_normal[size_t(q) * D + i] = best_n[i];
-    if (p.out_point) {
-      float pt[D];
-      if (best_leaf != kNoHit) ray_at<D>(r.o, r.d, best_t, pt);
-      else
-#pragma unroll
-        for (int i = 0; i < D; ++i) pt[i] = 0.f;
-#pragma unroll
-      for (int i = 0; i < D; ++i) p.out_point[size_t(q) * D + i] = pt[i];
+    if (live) {
+      bool done = false;
+      // Descend interior child-pair records until a leaf comes up.
+      while (!(L.code & kLeafBit)) {
+        float rec[NL::vec * 4];
+        load_vec<NL::vec>(p.nodes + size_t(L.code) * NL::vec, rec);
+        const uint32_t ca = __float_as_uint(rec[4 * D]);
+        const uint32_t cb = __float_as_uint(rec[4 * D + 1]);
+        float ta, tb;
+        const bool pa = test_box(rec, rec + D, ta);
+        const bool pb = test_box(rec + 2 * D, rec + 3 * D, tb);
+        if (STATS) L.v_nodes += 2;
+        if (pa && pb) {
+          // Reference order: child_a waits, child_b goes first. Near-first:
+          // the smaller entry goes first.
+          const bool a_first = (REF || !kNearest) ? false : (ta <= tb);
+          s_code[L.sp * kThreads + tid] = a_first ? cb : ca;
+          s_t[L.sp * kThreads + tid] = a_first ? tb : ta;
+          ++L.sp;
+          L.code = a_first ? ca : cb;
+        } else if (pa) {
+          L.code = ca;
+        } else if (pb) {
+          L.code = cb;
+        } else if (!pop()) {
+          done = true;
+          break;
+        }
+      }
+      if (!done) {
+        leaf();
+        done = !pop();
+      }
+      if (done) {
+        finish();
+        live = false;
+      }
     }
-  } else if constexpr (kList) {
-    // Entries past min(count, k) are left as they were.
-    p.out_count[q] = count;
-  } else {
-    if (!p.fill) p.out_count[q] = count;
-  }
-  if (STATS) {
-    c_vis += v_nodes;
-    c_nar += v_nar;
-    c_hit += v_hit;
-    if (p.query_stats) {
-      p.query_stats[size_t(q) * 4 + 0] = v_nodes;
-      p.query_stats[size_t(q) * 4 + 1] = v_nodes;
-      p.query_stats[size_t(q) * 4 + 2] = v_nar;
-      p.query_stats[size_t(q) * 4 + 3] = v_hit;
-    }
-  }
-}
-
-template <int D, int N, int K, bool REF, bool STATS>
-__global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
-  __shared__ uint32_t s_code[kStack][kThreads];
-  __shared__ float s_t[kStack][kThreads];
-  const int tid = threadIdx.x;
-  const int lane = tid & 31;
-  unsigned long long c_vis = 0, c_nar = 0, c_hit = 0;
-  for (;;) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(p.counter, 32u);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= p.n) break;
-    const uint32_t q = base + lane;
-    if (q < p.n) run_query<D, N, K, REF, STATS>(p, q, tid, s_code, s_t, c_vis, c_nar, c_hit);
   }
   if (STATS) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      c_vis += __shfl_down_sync(0xffffffffu, c_vis, o);
-      c_nar += __shfl_down_sync(0xffffffffu, c_nar, o);
-      c_hit += __shfl_down_sync(0xffffffffu, c_hit, o);
+      c_vis += __shfl_down_sync(FULL, c_vis, o);
+      c_nar += __shfl_down_sync(FULL, c_nar, o);
+      c_hit += __shfl_down_sync(FULL, c_hit, o);
     }
     if (lane == 0 && p.stats) {
       atomicAdd(p.stats + 0, c_vis);
@@ -476,6 +530,7 @@ struct RefitLeaf {
 };
 
 struct RefitParams {
+  int* nonfinite;  // set when a refit box is not finite
   float4* nodes;
   float4* prims;
   float* root_box;
@@ -542,6 +597,10 @@ template <int D, int N> __global__ void __launch_bounds__(256) refit_kernel(cons
 #pragma unroll
     for (int i = 0; i < D; ++i) { lo[i] = fminf(lo[i], plo[i]); hi[i] = fmaxf(hi[i], phi[i]); }
   }
+  bool fin = true;
+#pragma unroll
+  for (int i = 0; i < D; ++i) fin = fin && isfinite(lo[i]) && isfinite(hi[i]);
+  if (!fin) atomicOr(p.nonfinite, 1);
   uint32_t parent = L.parent;
   store_slot<D>(p, parent, lo, hi);
   while (parent != kNoHit) {

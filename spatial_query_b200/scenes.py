@@ -173,10 +173,10 @@ def terrain_scene(seed: int = 1, nx: int = 1024, ny: int = 512, n_coherent: int 
     rng = Rng(seed)
     verts, waves = heightfield(rng, nx, ny, 1.0, 1.0, 20.0, 0.5, 16.0, 512.0)
     tris = grid_triangles(verts)
-    n_coh = nx * ny // 2 if n_coherent is None else n_coherent
-    n_inc = nx * ny // 2 if n_incoherent is None else n_incoherent
-    # Coherent: one ray per camera-grid cell centre over a 1024 x 512 grid
-    # (sub-sampled evenly when n_coh is smaller than the grid).
+    n_coh = nx * ny if n_coherent is None else n_coherent
+    n_inc = nx * ny if n_incoherent is None else n_incoherent
+    # Coherent: one ray per camera-grid cell centre over the nx x ny grid
+    # (524,288 at full size; sub-sampled evenly when n_coh is smaller).
     cam = np.arange(n_coh, dtype=np.int64) * (nx * ny) // max(n_coh, 1)
     cx = (cam % nx).astype(np.float64) + 0.5
     cy = (cam // nx).astype(np.float64) + 0.5
