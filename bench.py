@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--order", default="near_first", choices=["near_first", "reference"])
+    ap.add_argument("--order", default="reference", choices=["near_first", "reference"])
     ap.add_argument("--rays", type=int, default=1 << 20,
                     help="rays per step (half coherent, half incoherent); the metric is quoted at 1,048,576")
     return ap.parse_args()
@@ -241,6 +241,7 @@ def main():
     # Instrumented run (untimed): per-batch counters for the algorithmic bytes.
     st = scene.raycast_nearest_d(d_rays, n, s["max_toi"], d_leaf, d_toi, d_nrm, stats=True)
     torch.cuda.synchronize()
+    replayed = ctx.last_replay_count if args.order == "near_first" else 0
     fetches = (st["nodes_visited"] - n) // 2          # child-pair records read
     alg_bytes = (fetches * info["node_record_bytes"] + st["narrow_tests"] * info["prim_record_bytes"]
                  + n * (RAY_BYTES + OUT_BYTES))
@@ -319,6 +320,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded height field and rays)",
             "config": {"workload": WORKLOAD, "path": f"plain GPU traversal, {args.order} order",
+                       "replayed_in_reference_order": int(replayed),
                        "l2": "flushed between steps (256 MiB write, outside the timed events)",
                        "parallelism": f"replicated scene, rays sharded per rank (dp{world})",
                        "tree": {"nodes": info["n_nodes"], "depth": info["max_depth"],

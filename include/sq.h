@@ -55,9 +55,11 @@ extern "C" {
 #define SQ_NARROW_SPHERE_NEAR 2 /* leaf = centre[D],radius; near root only (tests/gpu.rs:92-106) */
 #define SQ_NARROW_TRIANGLE 3    /* leaf = v0,v1,v2 (D = 3); Moeller-Trumbore (viewport-lib-query/src/lib.rs:295-320) */
 
-/* Traversal order of nearest queries. */
-#define SQ_ORDER_NEAR_FIRST 0   /* visit the child with the smaller slab entry first (fewest nodes) */
-#define SQ_ORDER_REFERENCE 1    /* the crate's own order (accel/bvh.rs:119-120): replays the CPU step for step */
+/* Traversal order of nearest queries (sq_ctx_set_order). */
+#define SQ_ORDER_NEAR_FIRST 0   /* visit the child with the smaller slab entry first; a query whose answer
+                                   could depend on the order is answered again in the reference order */
+#define SQ_ORDER_REFERENCE 1    /* the default: the crate's own order (accel/bvh.rs:119-120), replaying
+                                   the CPU's decisions step for step */
 
 typedef struct sq_ctx sq_ctx;
 typedef struct sq_bvh sq_bvh;
@@ -124,11 +126,21 @@ const char* sq_ctx_last_error(const sq_ctx* ctx);
 void* sq_ctx_stream(sq_ctx* ctx);
 int32_t sq_ctx_set_stream(sq_ctx* ctx, void* stream);
 int32_t sq_ctx_synchronize(sq_ctx* ctx);
-/* Nearest-query order (SQ_ORDER_*) and persistent-grid blocks per SM (0 = occupancy). */
+/* Nearest-query order (SQ_ORDER_*, default SQ_ORDER_REFERENCE) and
+ * persistent-grid blocks per SM (0 = occupancy). */
 int32_t sq_ctx_set_order(sq_ctx* ctx, int32_t order);
 int32_t sq_ctx_set_blocks_per_sm(sq_ctx* ctx, int32_t blocks);
+/* Near-first nearest queries are answered again in the reference order when
+ * their answer could depend on the visiting order: when a hit lies before
+ * its primitive's own AABB entry, or when a node pruned by the limit had its
+ * entry within `window` (relative, default 2^-16) past the final limit. */
+int32_t sq_ctx_set_replay_window(sq_ctx* ctx, float window);
 /* Kernels this context has launched so far. */
 uint64_t sq_ctx_launch_count(const sq_ctx* ctx);
+/* How many queries of the last near-first launch were answered again, in the
+ * same launch, in the reference order because their answer could depend on
+ * the visiting order (waits for the context's stream). */
+int32_t sq_ctx_last_replay_count(sq_ctx* ctx, uint32_t* out);
 
 /* ---- host tree build -------------------------------------------------------
  * tree::build (accel/tree.rs:39-49, 112-163): the median-split tree the
@@ -208,6 +220,111 @@ int32_t sq_overlap(sq_ctx* ctx, const sq_bvh* bvh, const float* regions, uint32_
                    uint64_t* offsets, uint32_t* leaves, uint64_t leaf_capacity, uint64_t* total);
 int32_t sq_overlap_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_regions, uint32_t n, const sq_filter* filter,
                      uint64_t* d_offsets, uint32_t* d_leaves, uint64_t leaf_capacity, uint64_t* total);
+
+/* ---- two-level scenes (accel/tlas.rs) -------------------------------------
+ * A Tlas over instances of one kind. Mesh instances (D = 3) reference a BLAS
+ * of a shared BLAS set and carry a uniform scale: the instance's local test is
+ * a nearest query in the mesh tree with the origin divided by the scale and
+ * max_toi / scale, the toi scaled back (the provider of the benchmark's
+ * instanced scene; Isometry itself is rigid, maths/isometry.rs:14-25). Box
+ * instances are the oriented boxes of tests/two_level.rs:42-113; ball
+ * instances the balls of tests/shape_overlap.rs:289-342. Rays are world-space;
+ * each instance maps them to local space (tlas.rs:459-481). */
+#define SQ_INSTANCE_MESH 0 /* param: scale; blas_id per instance */
+#define SQ_INSTANCE_BOX 1  /* param: half-extents[D] */
+#define SQ_INSTANCE_BALL 2 /* param: radius */
+
+typedef struct sq_blas_set sq_blas_set;
+typedef struct sq_tlas sq_tlas;
+typedef struct sq_graph sq_graph;
+
+/* Triangle meshes, each with its host tree (Bvh::build per mesh). Trees are
+ * concatenated: mesh b owns nodes [node_offsets[b], node_offsets[b+1]) with
+ * child indices local to the mesh, and triangles [tri_offsets[b],
+ * tri_offsets[b+1]) of `tris` (9 floats each, in mesh leaf order) with
+ * prim_indices local to the mesh. A hit's sub-object is the mesh-local
+ * triangle index. */
+int32_t sq_blas_set_upload(sq_ctx* ctx, uint32_t n_blas, const uint32_t* node_offsets, const float* node_bounds,
+                           const uint32_t* child_a, const uint32_t* child_b, const uint32_t* prim_count,
+                           const uint32_t* tri_offsets, const uint32_t* prim_indices, const float* tris,
+                           sq_blas_set** out);
+int32_t sq_blas_set_destroy(sq_blas_set* blas);
+
+/* World AABBs of instances (Isometry::transform_aabb of the local AABB,
+ * maths/isometry.rs:84-97): the boxes Tlas::build's tree is built over
+ * (tlas.rs:483-487). rot is n*D*D row-major, trans n*D. */
+int32_t sq_instance_world_aabbs(int32_t dim, int32_t kind, uint32_t n, const float* rot, const float* trans,
+                                const float* param, const uint32_t* blas_id, const sq_blas_set* blas,
+                                float* out_aabbs);
+
+/* Tlas::build's result uploaded (tlas.rs:35-45): the tree over the instance
+ * world AABBs as tree::Node arrays and its instance order. */
+int32_t sq_tlas_upload(sq_ctx* ctx, int32_t dim, int32_t kind, uint32_t n_inst, const float* rot,
+                       const float* trans, const float* param, const uint32_t* blas_id, const sq_blas_set* blas,
+                       uint32_t n_nodes, const float* node_bounds, const uint32_t* child_a,
+                       const uint32_t* child_b, const uint32_t* prim_count, const uint32_t* inst_indices,
+                       const uint64_t* layers, const uint32_t* sub_objects, sq_tlas** out);
+int32_t sq_tlas_destroy(sq_tlas* tlas);
+
+/* Tlas::refit (tlas.rs:49-54) on the device: new rotations (may be NULL),
+ * translations and instance parameters (may be NULL: a deforming provider's
+ * new local AABBs) per instance id, then the bottom-up pass. The _d form takes
+ * device pointers, any of them NULL, and per-instance translation steps
+ * (delta) added in place. */
+int32_t sq_tlas_refit(sq_ctx* ctx, sq_tlas* tlas, const float* rot, const float* trans, const float* param);
+int32_t sq_tlas_refit_d(sq_ctx* ctx, sq_tlas* tlas, const float* d_rot, const float* d_trans, const float* d_delta,
+                        const float* d_param);
+/* Node bounds in host-tree order and instance world AABBs in id order (either may be NULL). */
+int32_t sq_tlas_read_bounds(sq_ctx* ctx, const sq_tlas* tlas, float* node_bounds, float* world_aabbs);
+/* Tlas::needs_rebuild (tlas.rs:58-60). */
+int32_t sq_tlas_needs_rebuild(sq_ctx* ctx, const sq_tlas* tlas, float factor, int32_t* out);
+
+/* Tlas queries (tlas.rs:82-431): same layouts and semantics as the
+ * single-level ones; leaf = instance index. */
+int32_t sq_tlas_raycast_nearest(sq_ctx* ctx, const sq_tlas* tlas, const float* rays, uint32_t n, float max_toi,
+                                const float* max_toi_per_query, const sq_filter* filter, const sq_hits* out,
+                                sq_query_stats* stats);
+int32_t sq_tlas_raycast_all(sq_ctx* ctx, const sq_tlas* tlas, const float* rays, uint32_t n, float max_toi,
+                            const float* max_toi_per_query, const sq_filter* filter, const sq_hit_lists* out);
+int32_t sq_tlas_raycast_crossings(sq_ctx* ctx, const sq_tlas* tlas, const float* rays, uint32_t n, float max_toi,
+                                  const float* max_toi_per_query, const sq_filter* filter, const sq_hit_lists* out);
+int32_t sq_tlas_shapecast_nearest(sq_ctx* ctx, const sq_tlas* tlas, const float* casts, uint32_t n, float max_toi,
+                                  const float* max_toi_per_query, const sq_filter* filter, const sq_hits* out);
+int32_t sq_tlas_shapecast_all(sq_ctx* ctx, const sq_tlas* tlas, const float* casts, uint32_t n, float max_toi,
+                              const float* max_toi_per_query, const sq_filter* filter, const sq_hit_lists* out);
+int32_t sq_tlas_overlap(sq_ctx* ctx, const sq_tlas* tlas, const float* regions, uint32_t n, const sq_filter* filter,
+                        uint64_t* offsets, uint32_t* leaves, uint64_t leaf_capacity, uint64_t* total);
+
+/* One persistent launch over a mixed batch (device pointers): nearest rays,
+ * nearest shape casts and overlap regions. Overlaps report the full count
+ * and the first region_k instances in ascending order. */
+typedef struct sq_mixed_batch {
+  const float* rays;
+  uint32_t n_rays;
+  float ray_max_toi;
+  const float* ray_max_toi_per_query;
+  sq_hits ray_hits;
+  const float* casts;
+  uint32_t n_casts;
+  float cast_max_toi;
+  const float* cast_max_toi_per_query;
+  sq_hits cast_hits;
+  const float* regions;
+  uint32_t n_regions;
+  uint32_t region_k;
+  uint32_t* region_count;
+  uint32_t* region_leaves;
+} sq_mixed_batch;
+int32_t sq_tlas_mixed_d(sq_ctx* ctx, const sq_tlas* tlas, const sq_mixed_batch* batch, const sq_filter* filter);
+
+/* ---- CUDA graphs -------------------------------------------------------------
+ * Records the device-pointer calls made on the context's stream between
+ * begin and end (e.g. one frame: sq_tlas_refit_d + sq_tlas_mixed_d) and
+ * replays them with one launch. Host-buffer calls cannot be recorded. */
+int32_t sq_graph_begin(sq_ctx* ctx);
+int32_t sq_graph_end(sq_ctx* ctx, sq_graph** out);
+int32_t sq_graph_launch(sq_ctx* ctx, const sq_graph* graph);
+int32_t sq_graph_destroy(sq_graph* graph);
 
 #ifdef __cplusplus
 }

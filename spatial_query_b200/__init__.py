@@ -69,6 +69,13 @@ class _Stats(C.Structure):
                 ("hits", C.c_uint64)]
 
 
+class _Mixed(C.Structure):
+    _fields_ = [("rays", P), ("n_rays", C.c_uint32), ("ray_max_toi", C.c_float), ("ray_max_toi_per_query", P),
+                ("ray_hits", _Hits), ("casts", P), ("n_casts", C.c_uint32), ("cast_max_toi", C.c_float),
+                ("cast_max_toi_per_query", P), ("cast_hits", _Hits), ("regions", P), ("n_regions", C.c_uint32),
+                ("region_k", C.c_uint32), ("region_count", P), ("region_leaves", P)]
+
+
 class _Info(C.Structure):
     _fields_ = [("dim", C.c_int32), ("narrow", C.c_int32), ("n_nodes", C.c_uint32), ("n_prims", C.c_uint32),
                 ("max_depth", C.c_uint32), ("n_interior", C.c_uint32), ("device_bytes", C.c_uint64),
@@ -89,6 +96,8 @@ SIGNATURES = {
     "sq_ctx_set_order": (C.c_int32, [P, C.c_int32]),
     "sq_ctx_set_blocks_per_sm": (C.c_int32, [P, C.c_int32]),
     "sq_ctx_launch_count": (C.c_uint64, [P]),
+    "sq_ctx_last_replay_count": (C.c_int32, [P, C.POINTER(C.c_uint32)]),
+    "sq_ctx_set_replay_window": (C.c_int32, [P, C.c_float]),
     "sq_tree_build": (C.c_int32, [C.c_int32, C.c_uint32, P, C.c_int32, C.c_uint32, P, P, P, P, P, P]),
     "sq_prim_aabbs": (C.c_int32, [C.c_int32, C.c_int32, C.c_uint32, P, P]),
     "sq_bvh_upload": (C.c_int32, [P, C.c_int32, C.c_int32, C.c_uint32, P, P, P, P, C.c_uint32, P, P, C.c_uint32,
@@ -110,7 +119,30 @@ SIGNATURES = {
     "sq_shapecast_all_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P]),
     "sq_overlap": (C.c_int32, [P, P, P, C.c_uint32, P, P, P, C.c_uint64, C.POINTER(C.c_uint64)]),
     "sq_overlap_d": (C.c_int32, [P, P, P, C.c_uint32, P, P, P, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "sq_blas_set_upload": (C.c_int32, [P, C.c_uint32, P, P, P, P, P, P, P, P, C.POINTER(P)]),
+    "sq_blas_set_destroy": (C.c_int32, [P]),
+    "sq_instance_world_aabbs": (C.c_int32, [C.c_int32, C.c_int32, C.c_uint32, P, P, P, P, P, P]),
+    "sq_tlas_upload": (C.c_int32, [P, C.c_int32, C.c_int32, C.c_uint32, P, P, P, P, P, C.c_uint32, P, P, P, P, P,
+                                   P, P, C.POINTER(P)]),
+    "sq_tlas_destroy": (C.c_int32, [P]),
+    "sq_tlas_refit": (C.c_int32, [P, P, P, P, P]),
+    "sq_tlas_refit_d": (C.c_int32, [P, P, P, P, P, P]),
+    "sq_tlas_read_bounds": (C.c_int32, [P, P, P, P]),
+    "sq_tlas_needs_rebuild": (C.c_int32, [P, P, C.c_float, C.POINTER(C.c_int32)]),
+    "sq_tlas_raycast_nearest": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P, P]),
+    "sq_tlas_raycast_all": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P]),
+    "sq_tlas_raycast_crossings": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P]),
+    "sq_tlas_shapecast_nearest": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P]),
+    "sq_tlas_shapecast_all": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P]),
+    "sq_tlas_overlap": (C.c_int32, [P, P, P, C.c_uint32, P, P, P, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "sq_tlas_mixed_d": (C.c_int32, [P, P, P, P]),
+    "sq_graph_begin": (C.c_int32, [P]),
+    "sq_graph_end": (C.c_int32, [P, C.POINTER(P)]),
+    "sq_graph_launch": (C.c_int32, [P, P]),
+    "sq_graph_destroy": (C.c_int32, [P]),
 }
+
+INSTANCE = {"mesh": 0, "box": 1, "ball": 2}
 
 
 def lib():
@@ -234,9 +266,9 @@ class Context:
         self.device = device
 
     def close(self):
-        if getattr(self, "h", None):
-            lib().sq_ctx_destroy(self.h)
-            self.h = None
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.sq_ctx_destroy(self.h)
+        self.h = None
 
     def __del__(self):
         self.close()
@@ -247,6 +279,9 @@ class Context:
 
     def set_order(self, order: int):
         self.check(lib().sq_ctx_set_order(self.h, order), "set_order")
+
+    def set_replay_window(self, window: float):
+        self.check(lib().sq_ctx_set_replay_window(self.h, window), "set_replay_window")
 
     def set_blocks_per_sm(self, blocks: int):
         self.check(lib().sq_ctx_set_blocks_per_sm(self.h, blocks), "set_blocks_per_sm")
@@ -264,6 +299,41 @@ class Context:
     @property
     def launch_count(self) -> int:
         return int(lib().sq_ctx_launch_count(self.h))
+
+    @property
+    def last_replay_count(self) -> int:
+        """Queries of the last near-first nearest launch answered again in the
+        reference order."""
+        out = C.c_uint32(0)
+        self.check(lib().sq_ctx_last_replay_count(self.h, C.byref(out)), "last_replay_count")
+        return int(out.value)
+
+    def graph_begin(self):
+        """Start recording the device-pointer calls made on this context."""
+        self.check(lib().sq_graph_begin(self.h), "graph_begin")
+
+    def graph_end(self) -> "Graph":
+        g = P()
+        self.check(lib().sq_graph_end(self.h, C.byref(g)), "graph_end")
+        return Graph(self, g)
+
+
+class Graph:
+    """A recorded sequence of device calls, replayed with one launch."""
+
+    def __init__(self, ctx: Context, h):
+        self.ctx, self.h = ctx, h
+
+    def launch(self):
+        self.ctx.check(lib().sq_graph_launch(self.ctx.h, self.h), "graph_launch")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sq_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 @dataclass
@@ -322,9 +392,9 @@ class DeviceBvh:
         self.tree = tree
 
     def close(self):
-        if getattr(self, "h", None):
-            lib().sq_bvh_destroy(self.h)
-            self.h = None
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.sq_bvh_destroy(self.h)
+        self.h = None
 
     def __del__(self):
         self.close()
@@ -529,3 +599,193 @@ class GpuRaycaster:
 
     def overlap(self, regions, **kw):
         return self.scene.overlap(regions, **kw)
+
+
+# ---------------------------------------------------------------------------
+# Two-level scenes (accel/tlas.rs)
+# ---------------------------------------------------------------------------
+
+class BlasSet:
+    """Triangle meshes with their own host trees, uploaded once and shared by
+    every mesh instance (the lower level of a two-level scene)."""
+
+    def __init__(self, ctx: Context, meshes: list, threads: int = 0):
+        self.ctx = ctx
+        self.trees = []
+        node_off, tri_off = [0], [0]
+        bounds, ca, cb, pc, pi, tris = [], [], [], [], [], []
+        for m in meshes:
+            g = Geometry("tris", 3, m)
+            t = HostBvh.build(g, threads)
+            self.trees.append(t)
+            bounds.append(t.bounds.reshape(-1, 6))
+            ca.append(t.child_a)
+            cb.append(t.child_b)
+            pc.append(t.prim_count)
+            pi.append(t.prim_indices[: g.leaf_count])
+            tris.append(g.prims)
+            node_off.append(node_off[-1] + t.node_count)
+            tri_off.append(tri_off[-1] + g.leaf_count)
+        cat = lambda xs, dt, shape: (np.ascontiguousarray(np.concatenate(xs), dtype=dt) if xs and sum(len(x) for x in xs)
+                                     else np.zeros(shape, dt))
+        self._arrays = [np.asarray(node_off, np.uint32), cat(bounds, np.float32, (1, 6)), cat(ca, np.uint32, 1),
+                        cat(cb, np.uint32, 1), cat(pc, np.uint32, 1), np.asarray(tri_off, np.uint32),
+                        cat(pi, np.uint32, 1), cat(tris, np.float32, (1, 9))]
+        h = P()
+        a = self._arrays
+        ctx.check(lib().sq_blas_set_upload(ctx.h, len(meshes), _p(a[0]), _p(a[1]), _p(a[2]), _p(a[3]), _p(a[4]),
+                                           _p(a[5]), _p(a[6]), _p(a[7]), C.byref(h)), "sq_blas_set_upload")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sq_blas_set_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def instance_world_aabbs(kind: str, dim: int, rot, trans, param, blas_id=None, blas: BlasSet | None = None):
+    n = len(trans)
+    rot, trans, param = _f32(rot), _f32(trans), _f32(param)
+    bid = None if blas_id is None else np.ascontiguousarray(blas_id, dtype=np.uint32)
+    out = np.empty((n, 2 * dim), np.float32)
+    rc = lib().sq_instance_world_aabbs(dim, INSTANCE[kind], n, _p(rot), _p(trans), _p(param), _p(bid),
+                                       blas.h if blas else None, _p(out))
+    if rc:
+        raise SqError(rc, "sq_instance_world_aabbs")
+    return out
+
+
+class DeviceTlas:
+    """Tlas::build over instances, uploaded (sq_tlas_upload)."""
+
+    def __init__(self, ctx: Context, kind: str, dim: int, rot, trans, param, blas_id=None, blas: BlasSet | None = None,
+                 layers=None, sub_objects=None, threads: int = 0):
+        self.ctx, self.kind, self.dim, self.blas = ctx, kind, dim, blas
+        self.rot, self.trans, self.param = _f32(rot), _f32(trans), _f32(param)
+        self.blas_id = None if blas_id is None else np.ascontiguousarray(blas_id, dtype=np.uint32)
+        self.n = len(self.trans)
+        world = instance_world_aabbs(kind, dim, self.rot, self.trans, self.param, self.blas_id, blas)
+        self.tree = HostBvh.build_from_aabbs(dim, world, threads)
+        self._layers = None if layers is None else np.ascontiguousarray(layers, dtype=np.uint64)
+        self._sub = None if sub_objects is None else np.ascontiguousarray(sub_objects, dtype=np.uint32)
+        t = self.tree
+        nn = t.node_count
+        z = np.zeros(4, np.uint32)
+        h = P()
+        ctx.check(lib().sq_tlas_upload(ctx.h, dim, INSTANCE[kind], self.n, _p(self.rot), _p(self.trans),
+                                       _p(self.param), _p(self.blas_id), blas.h if blas else None, nn,
+                                       _p(t.bounds if nn else z), _p(t.child_a if nn else z),
+                                       _p(t.child_b if nn else z), _p(t.prim_count if nn else z),
+                                       _p(t.prim_indices if nn else z), _p(self._layers), _p(self._sub), C.byref(h)),
+                  "sq_tlas_upload")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sq_tlas_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def refit(self, trans, rot=None, param=None):
+        self.trans = _f32(trans)
+        r = None if rot is None else _f32(rot)
+        pr = None if param is None else _f32(param)
+        self.ctx.check(lib().sq_tlas_refit(self.ctx.h, self.h, _p(r), _p(self.trans), _p(pr)), "sq_tlas_refit")
+
+    def refit_d(self, d_rot=None, d_trans=None, d_delta=None, d_param=None):
+        self.ctx.check(lib().sq_tlas_refit_d(self.ctx.h, self.h, _p(d_rot), _p(d_trans), _p(d_delta), _p(d_param)),
+                       "sq_tlas_refit_d")
+
+    def read_bounds(self):
+        nb = np.empty((max(self.tree.node_count, 1), 2 * self.dim), np.float32)
+        wa = np.empty((max(self.n, 1), 2 * self.dim), np.float32)
+        self.ctx.check(lib().sq_tlas_read_bounds(self.ctx.h, self.h, _p(nb), _p(wa)), "sq_tlas_read_bounds")
+        return nb[: self.tree.node_count], wa[: self.n]
+
+    def needs_rebuild(self, factor: float) -> bool:
+        out = C.c_int32(0)
+        self.ctx.check(lib().sq_tlas_needs_rebuild(self.ctx.h, self.h, factor, C.byref(out)), "needs_rebuild")
+        return bool(out.value)
+
+    def _nearest(self, fn, q, width, max_toi, mask, exclude, stats):
+        q = _f32(q).reshape(-1, width * self.dim)
+        n = q.shape[0]
+        per = np.ndim(max_toi) > 0
+        mt = _f32(max_toi) if per else None
+        h = Hits(np.empty(n, np.uint32), np.empty(n, np.float32), np.empty((n, self.dim), np.float32),
+                 np.empty((n, self.dim), np.float32), np.empty(n, np.uint32))
+        s = _Hits(_p(h.leaf), _p(h.toi), _p(h.sub_object), _p(h.normal), _p(h.point))
+        args = [self.ctx.h, self.h, _p(q), n, 0.0 if per else float(max_toi), _p(mt), _filter(mask, exclude),
+                C.byref(s)]
+        st = _Stats() if stats else None
+        if fn == "sq_tlas_raycast_nearest":
+            args.append(C.byref(st) if st else None)
+        self.ctx.check(getattr(lib(), fn)(*args), fn)
+        if st:
+            h.stats = _stats_dict(st)
+        return h
+
+    def _lists(self, fn, q, width, max_toi, k, mask, exclude):
+        q = _f32(q).reshape(-1, width * self.dim)
+        n = q.shape[0]
+        per = np.ndim(max_toi) > 0
+        mt = _f32(max_toi) if per else None
+        h = HitLists(np.empty(n, np.uint32), np.empty((n, k), np.uint32), np.empty((n, k), np.float32),
+                     np.empty((n, k, self.dim), np.float32), np.empty((n, k), np.uint32))
+        s = _Lists(k, _p(h.count), _p(h.leaf), _p(h.toi), _p(h.sub_object), _p(h.normal))
+        self.ctx.check(getattr(lib(), fn)(self.ctx.h, self.h, _p(q), n, 0.0 if per else float(max_toi), _p(mt),
+                                          _filter(mask, exclude), C.byref(s)), fn)
+        return h
+
+    def raycast_nearest(self, rays, max_toi, mask=None, exclude=None, stats=False) -> Hits:
+        return self._nearest("sq_tlas_raycast_nearest", rays, 2, max_toi, mask, exclude, stats)
+
+    def raycast_all(self, rays, max_toi, k=16, mask=None, exclude=None) -> HitLists:
+        return self._lists("sq_tlas_raycast_all", rays, 2, max_toi, k, mask, exclude)
+
+    def raycast_crossings(self, rays, max_toi, k=16, mask=None, exclude=None) -> HitLists:
+        return self._lists("sq_tlas_raycast_crossings", rays, 2, max_toi, k, mask, exclude)
+
+    def shapecast_nearest(self, casts, max_toi, mask=None, exclude=None) -> Hits:
+        return self._nearest("sq_tlas_shapecast_nearest", casts, 4, max_toi, mask, exclude, False)
+
+    def shapecast_all(self, casts, max_toi, k=16, mask=None, exclude=None) -> HitLists:
+        return self._lists("sq_tlas_shapecast_all", casts, 4, max_toi, k, mask, exclude)
+
+    def overlap(self, regions, mask=None, exclude=None, capacity=None):
+        regions = _f32(regions).reshape(-1, 2 * self.dim)
+        n = regions.shape[0]
+        cap = capacity if capacity is not None else max(4 * n, 1024)
+        while True:
+            offsets = np.empty(n + 1, np.uint64)
+            leaves = np.empty(max(cap, 1), np.uint32)
+            total = C.c_uint64(0)
+            rc = lib().sq_tlas_overlap(self.ctx.h, self.h, _p(regions), n, _filter(mask, exclude), _p(offsets),
+                                       _p(leaves), cap, C.byref(total))
+            if rc == SQ_ERR_CAPACITY:
+                cap = int(total.value)
+                continue
+            self.ctx.check(rc, "sq_tlas_overlap")
+            return offsets, leaves[: int(total.value)]
+
+    def mixed_d(self, rays=None, n_rays=0, ray_max_toi=0.0, ray_out=None, casts=None, n_casts=0, cast_max_toi=0.0,
+                cast_max_toi_per_query=None, cast_out=None, regions=None, n_regions=0, region_k=0, region_count=None,
+                region_leaves=None, mask=None, exclude=None):
+        """One persistent launch over device buffers (torch tensors). ray_out /
+        cast_out: dicts of leaf, toi, normal, point, sub tensors."""
+        ro = ray_out or {}
+        co = cast_out or {}
+        m = _Mixed(_p(rays), n_rays, ray_max_toi, None,
+                   _Hits(_p(ro.get("leaf")), _p(ro.get("toi")), _p(ro.get("sub")), _p(ro.get("normal")),
+                         _p(ro.get("point"))),
+                   _p(casts), n_casts, cast_max_toi, _p(cast_max_toi_per_query),
+                   _Hits(_p(co.get("leaf")), _p(co.get("toi")), _p(co.get("sub")), _p(co.get("normal")),
+                         _p(co.get("point"))),
+                   _p(regions), n_regions, region_k, _p(region_count), _p(region_leaves))
+        self.ctx.check(lib().sq_tlas_mixed_d(self.ctx.h, self.h, C.byref(m), _filter(mask, exclude)),
+                       "sq_tlas_mixed_d")

@@ -27,6 +27,8 @@ UNITS = [
     ("kernels_d3.cu", ["--fmad=false"]),
     ("kernels_d4.cu", ["--fmad=false"]),
     ("kernels_d6.cu", ["--fmad=false"]),
+    ("sq_tlas.cu", ["--fmad=false"]),
+    ("tlas_kernels.cu", ["--fmad=false"]),
     ("tree_build.cpp", []),
 ]
 

@@ -21,45 +21,9 @@
 #include <unordered_map>
 #include <vector>
 
-#include "../../include/sq.h"
-#include "traverse.cuh"
-
-namespace sq {
-bool kernel_set_d2(int narrow, KernelSet* out);
-bool kernel_set_d3(int narrow, KernelSet* out);
-bool kernel_set_d4(int narrow, KernelSet* out);
-bool kernel_set_d6(int narrow, KernelSet* out);
-}  // namespace sq
+#include "sq_internal.cuh"
 
 using namespace sq;
-
-namespace {
-
-constexpr uint32_t kCounterSlots = 4096;
-
-struct DevBuf {
-  void* p = nullptr;
-  size_t cap = 0;
-};
-
-}  // namespace
-
-struct sq_ctx {
-  int device = 0;
-  cudaStream_t own = nullptr;
-  cudaStream_t stream = nullptr;
-  std::string err;
-  int sm_count = 0;
-  int order = SQ_ORDER_NEAR_FIRST;
-  int blocks_per_sm = 0;
-  uint32_t* d_counters = nullptr;
-  uint32_t slot = 0;
-  unsigned long long* d_stats = nullptr;
-  DevBuf arena;
-  uint64_t launches = 0;
-  std::unordered_map<uint64_t, int> occ;  // (kernel, dynamic smem) -> resident blocks per SM
-};
-
 struct sq_bvh {
   int device = 0;
   int dim = 0;
@@ -86,100 +50,7 @@ struct sq_bvh {
 
 namespace {
 
-int32_t fail(sq_ctx* c, int32_t code, const std::string& msg) {
-  if (c) c->err = msg;
-  return code;
-}
-
-int32_t cuda_fail(sq_ctx* c, const char* what, cudaError_t e) {
-  return fail(c, SQ_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-#define CK(x)                                          \
-  do {                                                 \
-    cudaError_t e_ = (x);                              \
-    if (e_ != cudaSuccess) return cuda_fail(ctx, #x, e_); \
-  } while (0)
-
-bool kernel_set(int dim, int narrow, KernelSet* out) {
-  switch (dim) {
-    case 2: return kernel_set_d2(narrow, out);
-    case 3: return kernel_set_d3(narrow, out);
-    case 4: return kernel_set_d4(narrow, out);
-    case 6: return kernel_set_d6(narrow, out);
-    default: return false;
-  }
-}
-
-uint32_t stride_of(int dim, int narrow) {
-  switch (narrow) {
-    case SQ_NARROW_AABB: return 2 * dim;
-    case SQ_NARROW_SPHERE:
-    case SQ_NARROW_SPHERE_NEAR: return dim + 1;
-    case SQ_NARROW_TRIANGLE: return 9;
-    default: return 0;
-  }
-}
-
-uint32_t prim_vec(int dim, int narrow) {
-  uint32_t payload = narrow == SQ_NARROW_AABB ? 2 * dim : (narrow == SQ_NARROW_TRIANGLE ? 9 : dim + 1);
-  return (payload + 1 + 3) / 4;
-}
-
-uint32_t node_vec(int dim) { return (4 * dim + 2 + 3) / 4; }
-
-int32_t arena_reserve(sq_ctx* ctx, size_t bytes) {
-  if (ctx->arena.cap >= bytes) return SQ_OK;
-  if (ctx->arena.p) {
-    CK(cudaStreamSynchronize(ctx->stream));
-    CK(cudaFree(ctx->arena.p));
-    ctx->arena.p = nullptr;
-    ctx->arena.cap = 0;
-  }
-  size_t cap = std::max<size_t>(bytes, size_t(1) << 20);
-  CK(cudaMalloc(&ctx->arena.p, cap));
-  ctx->arena.cap = cap;
-  return SQ_OK;
-}
-
-// Carves 256-byte-aligned pieces out of the arena.
-struct Carve {
-  size_t off = 0;
-  size_t take(size_t bytes) {
-    size_t o = off;
-    off += (bytes + 255) & ~size_t(255);
-    return o;
-  }
-};
-
-int occupancy(sq_ctx* ctx, const void* fn, size_t smem) {
-  const uint64_t key = uint64_t(uintptr_t(fn)) * 131 + smem;
-  auto it = ctx->occ.find(key);
-  if (it != ctx->occ.end()) return it->second;
-  int nb = 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kThreads, smem) != cudaSuccess || nb < 1) nb = 1;
-  ctx->occ[key] = nb;
-  return nb;
-}
-
-// The persistent grid: (resident blocks per SM) x (SM count), no more blocks
-// than the queries need. The traversal stack is dynamic shared memory sized
-// to the tree depth, so shallow trees leave room for more resident warps.
-int32_t launch_persistent(sq_ctx* ctx, const void* fn, QueryParams& p, uint32_t depth) {
-  uint32_t* ctr = ctx->d_counters + (ctx->slot++ % kCounterSlots);
-  CK(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), ctx->stream));
-  p.counter = ctr;
-  p.stack = int(std::max<uint32_t>(depth, 1));
-  const size_t smem = size_t(p.stack) * kThreads * 8;
-  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  int bps = ctx->blocks_per_sm > 0 ? ctx->blocks_per_sm : occupancy(ctx, fn, smem);
-  uint64_t want = (uint64_t(p.n) + kThreads - 1) / kThreads;
-  uint64_t grid = std::min<uint64_t>(uint64_t(ctx->sm_count) * bps, std::max<uint64_t>(want, 1));
-  void* args[] = {&p};
-  CK(cudaLaunchKernel(fn, dim3(unsigned(grid)), dim3(kThreads), args, smem, ctx->stream));
-  ctx->launches++;
-  return SQ_OK;
-}
+using namespace sqi;
 
 void base_params(const sq_bvh* b, const sq_filter* f, QueryParams& p) {
   std::memset(&p, 0, sizeof(p));
@@ -229,15 +100,16 @@ int32_t nearest_core(sq_ctx* ctx, const sq_bvh* b, bool cast, const float* d_q, 
   p.out_sub = o.sub_object;
   p.out_normal = o.normal;
   p.out_point = o.point;
-  const int ref = ctx->order == SQ_ORDER_REFERENCE ? 1 : 0;
-  const void* fn;
-  if (cast) {
-    fn = b->ks.cast_nearest[ref];
-  } else {
-    fn = b->ks.ray_nearest[ref][stats ? 1 : 0];
-    if (stats) p.stats = ctx->d_stats;
-  }
-  return launch_persistent(ctx, fn, p, b->depth);
+  const bool near_first = ctx->order != SQ_ORDER_REFERENCE;
+  const int st = stats ? 1 : 0;
+  if (stats && !cast) p.stats = ctx->d_stats;
+  const void* ref_fn = cast ? b->ks.cast_nearest[1] : b->ks.ray_nearest[1][st];
+  if (!near_first) return launch_persistent(ctx, ref_fn, p, b->depth, p.n);
+  CK(cudaMemsetAsync(ctx->d_replays, 0, sizeof(uint32_t), ctx->stream));
+  p.replay_count = ctx->d_replays;
+  p.window = ctx->window;
+  const void* near_fn = cast ? b->ks.cast_nearest[0] : b->ks.ray_nearest[0][st];
+  return launch_persistent(ctx, near_fn, p, b->depth, p.n);
 }
 
 int32_t list_core(sq_ctx* ctx, const sq_bvh* b, int kind, const float* d_q, uint32_t n, float max_toi,
@@ -268,7 +140,7 @@ int32_t list_core(sq_ctx* ctx, const sq_bvh* b, int kind, const float* d_q, uint
     fn = b->ks.ray_all[stats ? 1 : 0];
     if (stats) p.stats = ctx->d_stats;
   }
-  return launch_persistent(ctx, fn, p, b->depth);
+  return launch_persistent(ctx, fn, p, b->depth, p.n);
 }
 
 int32_t stats_begin(sq_ctx* ctx, sq_query_stats* st) {
@@ -317,6 +189,7 @@ extern "C" int32_t sq_ctx_create(int32_t device, sq_ctx** out) {
     fprintf(stderr, "sq_ctx_create: %s: %s\n", w, cudaGetErrorString(e));
     if (ctx->d_counters) cudaFree(ctx->d_counters);
     if (ctx->d_stats) cudaFree(ctx->d_stats);
+    if (ctx->d_replays) cudaFree(ctx->d_replays);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
     return SQ_ERR_CUDA;
@@ -329,6 +202,8 @@ extern "C" int32_t sq_ctx_create(int32_t device, sq_ctx** out) {
     return bail(e, "sm count");
   if ((e = cudaMalloc(&ctx->d_counters, kCounterSlots * sizeof(uint32_t))) != cudaSuccess) return bail(e, "counters");
   if ((e = cudaMalloc(&ctx->d_stats, 4 * sizeof(unsigned long long))) != cudaSuccess) return bail(e, "stats");
+  if ((e = cudaMalloc(&ctx->d_replays, sizeof(uint32_t))) != cudaSuccess) return bail(e, "replays");
+  if ((e = cudaMemset(ctx->d_replays, 0, sizeof(uint32_t))) != cudaSuccess) return bail(e, "replays");
   *out = ctx;
   return SQ_OK;
 }
@@ -338,6 +213,7 @@ extern "C" int32_t sq_ctx_destroy(sq_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->own) cudaStreamSynchronize(ctx->own);
   if (ctx->arena.p) cudaFree(ctx->arena.p);
+  if (ctx->d_replays) cudaFree(ctx->d_replays);
   if (ctx->d_counters) cudaFree(ctx->d_counters);
   if (ctx->d_stats) cudaFree(ctx->d_stats);
   if (ctx->own) cudaStreamDestroy(ctx->own);
@@ -374,6 +250,20 @@ extern "C" int32_t sq_ctx_set_blocks_per_sm(sq_ctx* ctx, int32_t blocks) {
 }
 
 extern "C" uint64_t sq_ctx_launch_count(const sq_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+extern "C" int32_t sq_ctx_set_replay_window(sq_ctx* ctx, float window) {
+  if (!ctx || !(window >= 0.f) || window > 1.f) return SQ_ERR_INVALID;
+  ctx->window = window;
+  return SQ_OK;
+}
+
+extern "C" int32_t sq_ctx_last_replay_count(sq_ctx* ctx, uint32_t* out) {
+  if (!ctx || !out) return SQ_ERR_INVALID;
+  *out = 0;
+  CK(cudaMemcpyAsync(out, ctx->d_replays, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SQ_OK;
+}
 
 // ============================================================================
 // upload / refit
@@ -693,7 +583,7 @@ int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint3
     p.n = n;
     p.out_count = d_counts;
     p.fill = 0;
-    int32_t rc = launch_persistent(ctx, b->ks.overlap, p, b->depth);
+    int32_t rc = launch_persistent(ctx, b->ks.overlap, p, b->depth, p.n);
     if (rc) return rc;
   }
   CK(cub::DeviceScan::ExclusiveScan(temp, temp_bytes, d_counts, (unsigned long long*)d_offsets, cuda::std::plus<>{},
@@ -713,7 +603,7 @@ int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint3
     p.fill = 1;
     p.csr_offsets = (const unsigned long long*)d_offsets;
     p.csr_leaves = d_leaves;
-    int32_t rc = launch_persistent(ctx, b->ks.overlap, p, b->depth);
+    int32_t rc = launch_persistent(ctx, b->ks.overlap, p, b->depth, p.n);
     if (rc) return rc;
   }
   return SQ_OK;

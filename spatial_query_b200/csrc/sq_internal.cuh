@@ -1,0 +1,160 @@
+// Internal declarations shared by the C ABI translation units: the context
+// object and the launch / staging helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/sq.h"
+#include "traverse.cuh"
+
+namespace sq {
+bool kernel_set_d2(int narrow, KernelSet* out);
+bool kernel_set_d3(int narrow, KernelSet* out);
+bool kernel_set_d4(int narrow, KernelSet* out);
+bool kernel_set_d6(int narrow, KernelSet* out);
+}  // namespace sq
+
+
+namespace sqi {
+
+constexpr uint32_t kCounterSlots = 4096;
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+}  // namespace sqi
+
+struct sq_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int sm_count = 0;
+  int order = SQ_ORDER_REFERENCE;  // exact by construction; near-first is opt-in
+  int blocks_per_sm = 0;
+  uint32_t* d_counters = nullptr;
+  uint32_t slot = 0;
+  unsigned long long* d_stats = nullptr;
+  sqi::DevBuf arena;
+  uint32_t* d_replays = nullptr;  // queries of the last near-first launch answered again in reference order
+  float window = 0x1p-16f;        // relative window past the limit that flags a pruned node
+  uint64_t launches = 0;
+  std::unordered_map<uint64_t, int> occ;  // (kernel, dynamic smem) -> resident blocks per SM
+};
+
+namespace sqi {
+
+using namespace sq;
+
+inline int32_t fail(sq_ctx* c, int32_t code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+inline int32_t cuda_fail(sq_ctx* c, const char* what, cudaError_t e) {
+  return fail(c, SQ_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(x)                                          \
+  do {                                                 \
+    cudaError_t e_ = (x);                              \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, #x, e_); \
+  } while (0)
+
+inline bool kernel_set(int dim, int narrow, KernelSet* out) {
+  switch (dim) {
+    case 2: return kernel_set_d2(narrow, out);
+    case 3: return kernel_set_d3(narrow, out);
+    case 4: return kernel_set_d4(narrow, out);
+    case 6: return kernel_set_d6(narrow, out);
+    default: return false;
+  }
+}
+
+inline uint32_t stride_of(int dim, int narrow) {
+  switch (narrow) {
+    case SQ_NARROW_AABB: return 2 * dim;
+    case SQ_NARROW_SPHERE:
+    case SQ_NARROW_SPHERE_NEAR: return dim + 1;
+    case SQ_NARROW_TRIANGLE: return 9;
+    default: return 0;
+  }
+}
+
+inline uint32_t prim_vec(int dim, int narrow) {
+  uint32_t payload = narrow == SQ_NARROW_AABB ? 2 * dim : (narrow == SQ_NARROW_TRIANGLE ? 9 : dim + 1);
+  return (payload + 1 + 3) / 4;
+}
+
+inline uint32_t node_vec(int dim) { return (4 * dim + 2 + 3) / 4; }
+
+inline int32_t arena_reserve(sq_ctx* ctx, size_t bytes) {
+  if (ctx->arena.cap >= bytes) return SQ_OK;
+  if (ctx->arena.p) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaFree(ctx->arena.p));
+    ctx->arena.p = nullptr;
+    ctx->arena.cap = 0;
+  }
+  size_t cap = std::max<size_t>(bytes, size_t(1) << 20);
+  CK(cudaMalloc(&ctx->arena.p, cap));
+  ctx->arena.cap = cap;
+  return SQ_OK;
+}
+
+// Carves 256-byte-aligned pieces out of the arena.
+struct Carve {
+  size_t off = 0;
+  size_t take(size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) & ~size_t(255);
+    return o;
+  }
+};
+
+inline int occupancy(sq_ctx* ctx, const void* fn, size_t smem) {
+  const uint64_t key = uint64_t(uintptr_t(fn)) * 131 + smem;
+  auto it = ctx->occ.find(key);
+  if (it != ctx->occ.end()) return it->second;
+  int nb = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kThreads, smem) != cudaSuccess || nb < 1) nb = 1;
+  ctx->occ[key] = nb;
+  return nb;
+}
+
+// The persistent grid: (resident blocks per SM) x (SM count), no more blocks
+// than the queries need. The traversal stack is dynamic shared memory sized
+// to the tree depth, so shallow trees leave room for more resident warps.
+// Launches a persistent kernel whose single parameter is *params (with its
+// counter and stack fields set here) on the context's stream.
+template <class Params>
+inline int32_t launch_persistent(sq_ctx* ctx, const void* fn, Params& p, uint32_t depth, uint64_t n);
+
+template <class Params>
+inline int32_t launch_persistent(sq_ctx* ctx, const void* fn, Params& p, uint32_t depth, uint64_t n) {
+  uint32_t* ctr = ctx->d_counters + (ctx->slot++ % kCounterSlots);
+  CK(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), ctx->stream));
+  p.counter = ctr;
+  p.stack = int(std::max<uint32_t>(depth, 1));
+  const size_t smem = size_t(p.stack) * kThreads * 8;
+  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  int bps = ctx->blocks_per_sm > 0 ? ctx->blocks_per_sm : occupancy(ctx, fn, smem);
+  uint64_t want = (n + kThreads - 1) / kThreads;
+  uint64_t grid = std::min<uint64_t>(uint64_t(ctx->sm_count) * bps, std::max<uint64_t>(want, 1));
+  void* args[] = {&p};
+  CK(cudaLaunchKernel(fn, dim3(unsigned(grid)), dim3(kThreads), args, smem, ctx->stream));
+  ctx->launches++;
+  return SQ_OK;
+}
+
+
+}  // namespace sqi

@@ -63,6 +63,8 @@ struct QueryParams {
   uint32_t* csr_leaves;
   unsigned long long* stats;
   uint32_t* query_stats;  // optional per-query counters [n][4] (u32)
+  uint32_t* replay_count;  // optional: queries answered again in the reference order
+  float window;            // relative window past the limit that flags a pruned node
   unsigned long long mask;
   long long exclude;
   const float* root_box;  // min[D], max[D] of the root (device memory: refit updates it)
@@ -91,6 +93,53 @@ template <int NV> __device__ __forceinline__ void load_vec(const float4* __restr
     dst[4 * j + 2] = v.z;
     dst[4 * j + 3] = v.w;
   }
+}
+
+// Near-first traversal visits nodes in another order than the reference. The
+// answers agree unless a primitive's hit rounds to before the slab entry of
+// its own leaf (possible for balls and triangles by a few ulps) and another
+// hit lies in between. A lane flags its query when it sees such a hit, or
+// when some node it pruned by the limit has an entry within a small relative
+// window (2^-16 by default) past the final limit (where an unseen primitive of that kind could
+// hide a hit no later than the answer; later hits cannot change it). A
+// flagged query is answered again at once, by the same lane, in the
+// reference order.
+__device__ __forceinline__ float near_limit(float limit, float window) {
+  return __fadd_rn(limit, __fadd_rn(__fmul_rn(fabsf(limit), window), 0x1p-20f));
+}
+
+// The slab entry of a primitive's own AABB for a ray or sweep (computed only
+// when the primitive is hit): a hit before it is a hit before every box that
+// encloses the primitive.
+template <int D, int N, bool CAST>
+__device__ __forceinline__ float prim_entry(const float* rec, const RayPre<D>& r, const float* pmin, const float* pmax,
+                                            bool fast) {
+  float lo[D], hi[D], te;
+  int ax;
+  const float inf = __int_as_float(0x7f800000);
+  if constexpr (N == kNarrowTri) {
+    tri_aabb(rec, rec + 3, rec + 6, lo, hi);
+  } else if constexpr (N == kNarrowSphere || N == kNarrowSphereNear) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      lo[i] = fsub(rec[i], rec[D]);
+      hi[i] = fadd(rec[i], rec[D]);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      lo[i] = rec[i];
+      hi[i] = rec[D + i];
+    }
+  }
+  if constexpr (CAST) {
+    if (fast) slab_grown_fast<D>(r, lo, hi, pmin, pmax, inf, te);
+    else slab_grown<D>(r, lo, hi, pmin, pmax, inf, te, ax);
+  } else {
+    if (fast) slab_fast<D>(r, lo, hi, inf, te);
+    else slab<D>(r, lo, hi, inf, te, ax);
+  }
+  return te;
 }
 
 // One primitive's ray test (QueryGeometry::test_ray for the built-in providers).
@@ -156,35 +205,43 @@ __device__ __forceinline__ bool narrow_overlap(const float* rec, const float* ql
 }
 
 // Sorted insertion into query q's bounded hit list (hit_ordering, stable:
-// an equal key goes after the entries already present).
+// an equal key goes after the entries already present). `count` is the full
+// number of hits so far; the first min(count, k) entries are kept.
 template <int D>
-__device__ __forceinline__ void list_insert(const QueryParams& p, uint32_t q, uint32_t& count, float t, uint32_t leaf,
-                                            const float* n) {
-  const uint32_t k = p.k;
+__device__ __forceinline__ void list_put(uint32_t k, uint32_t* o_leaf, float* o_toi, uint32_t* o_sub, float* o_nrm,
+                                         uint32_t q, uint32_t& count, float t, uint32_t leaf, uint32_t subv,
+                                         const float* n) {
   uint32_t m = count < k ? count : k;
   ++count;
   if (k == 0) return;
   const size_t base = size_t(q) * k;
   if (m == k) {
-    if (!hit_before(t, leaf, p.out_toi[base + k - 1], p.out_leaf[base + k - 1])) return;
+    if (!hit_before(t, leaf, o_toi[base + k - 1], o_leaf[base + k - 1])) return;
     m = k - 1;
   }
   uint32_t j = m;
-  while (j > 0 && hit_before(t, leaf, p.out_toi[base + j - 1], p.out_leaf[base + j - 1])) {
-    p.out_toi[base + j] = p.out_toi[base + j - 1];
-    p.out_leaf[base + j] = p.out_leaf[base + j - 1];
-    if (p.out_sub) p.out_sub[base + j] = p.out_sub[base + j - 1];
-    if (p.out_normal)
+  while (j > 0 && hit_before(t, leaf, o_toi[base + j - 1], o_leaf[base + j - 1])) {
+    o_toi[base + j] = o_toi[base + j - 1];
+    o_leaf[base + j] = o_leaf[base + j - 1];
+    if (o_sub) o_sub[base + j] = o_sub[base + j - 1];
+    if (o_nrm)
 #pragma unroll
-      for (int i = 0; i < D; ++i) p.out_normal[(base + j) * D + i] = p.out_normal[(base + j - 1) * D + i];
+      for (int i = 0; i < D; ++i) o_nrm[(base + j) * D + i] = o_nrm[(base + j - 1) * D + i];
     --j;
   }
-  p.out_toi[base + j] = t;
-  p.out_leaf[base + j] = leaf;
-  if (p.out_sub) p.out_sub[base + j] = p.sub ? __ldg(p.sub + leaf) : kNoHit;
-  if (p.out_normal)
+  o_toi[base + j] = t;
+  o_leaf[base + j] = leaf;
+  if (o_sub) o_sub[base + j] = subv;
+  if (o_nrm)
 #pragma unroll
-    for (int i = 0; i < D; ++i) p.out_normal[(base + j) * D + i] = n[i];
+    for (int i = 0; i < D; ++i) o_nrm[(base + j) * D + i] = n[i];
+}
+
+template <int D>
+__device__ __forceinline__ void list_insert(const QueryParams& p, uint32_t q, uint32_t& count, float t, uint32_t leaf,
+                                            const float* n) {
+  list_put<D>(p.k, p.out_leaf, p.out_toi, p.out_sub, p.out_normal, q, count, t, leaf,
+              p.sub ? __ldg(p.sub + leaf) : kNoHit, n);
 }
 
 // Per-lane traversal state of one query.
@@ -192,6 +249,9 @@ template <int D, int K> struct Lane {
   RayPre<D> r;
   float pmin[D], pmax[D];
   float limit;
+  float min_pruned;  // smallest entry among nodes pruned by the limit
+  uint32_t flag;     // a hit came before its own primitive's AABB entry
+  bool ref;          // this pass runs in the reference order (a replay)
   uint32_t q;
   uint32_t code;
   int sp;
@@ -232,20 +292,31 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   unsigned long long c_vis = 0, c_nar = 0, c_hit = 0;
   Lane<D, K> L;
   bool live = false, exhausted = false;
+  const uint32_t n_queries = p.n;
+  uint32_t replays = 0;
 
-  // Box test of one child (or the root) against the lane's query.
+  constexpr bool DETECT = kNearest && !REF;
+  const float kInf = __int_as_float(0x7f800000);
+
+  // Box test of one child (or the root) against the lane's query: the slab
+  // without the limit, then the entry against the limit (the same verdict as
+  // the reference's slab clipped to the limit, aabb.rs:118-148).
   auto test_box = [&](const float* lo, const float* hi, float& te) -> bool {
     if constexpr (K == kOverlap) {
       te = 0.f;
       return box_overlap<D>(lo, hi, L.r.o, L.r.d);  // region lo / hi sit in o / d
-    } else if constexpr (kCast) {
-      if (L.fast) return slab_grown_fast<D>(L.r, lo, hi, L.pmin, L.pmax, L.limit, te);
-      int ax;
-      return slab_grown<D>(L.r, lo, hi, L.pmin, L.pmax, L.limit, te, ax) && te <= L.limit;
     } else {
-      if (L.fast) return slab_fast<D>(L.r, lo, hi, L.limit, te);
+      bool geo;
       int ax;
-      return slab<D>(L.r, lo, hi, L.limit, te, ax) && te <= L.limit;
+      if constexpr (kCast) {
+        geo = L.fast ? slab_grown_fast<D>(L.r, lo, hi, L.pmin, L.pmax, kInf, te)
+                     : slab_grown<D>(L.r, lo, hi, L.pmin, L.pmax, kInf, te, ax);
+      } else {
+        geo = L.fast ? slab_fast<D>(L.r, lo, hi, kInf, te) : slab<D>(L.r, lo, hi, kInf, te, ax);
+      }
+      const bool pass = geo && te <= L.limit;
+      if (DETECT) L.min_pruned = fminf(L.min_pruned, (geo && !pass) ? te : kInf);
+      return pass;
     }
   };
 
@@ -257,6 +328,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
       L.code = s_code[L.sp * kThreads + tid];
       const float t = s_t[L.sp * kThreads + tid];
       if (!kNearest || t <= L.limit) return true;
+      if (DETECT) L.min_pruned = fminf(L.min_pruned, t);
     }
     return false;
   };
@@ -303,6 +375,8 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   // Loads query q and tests the root. False when the query is already done.
   auto start = [&](uint32_t q) -> bool {
     L.q = q;
+    L.flag = 0u;
+    L.min_pruned = kInf;
     const float* src = p.queries + size_t(q) * QW;
 #pragma unroll
     for (int i = 0; i < D; ++i) {
@@ -340,12 +414,13 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
     L.v_hit = 0;
     L.sp = 0;
     L.code = p.root_code;
-    float lo[D], hi[D], te;
+    float lo[D], hi[D];
 #pragma unroll
     for (int i = 0; i < D; ++i) {
       lo[i] = p.root_box[i];
       hi[i] = p.root_box[D + i];
     }
+    float te;
     return test_box(lo, hi, te);
   };
 
@@ -380,6 +455,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
             else h = narrow_cast<D, N>(rec, L.r, L.pmin, L.pmax, L.limit, t, nrm);
             if (h) {
               if (STATS) L.v_hit += 1;
+              if (DETECT && N != kNarrowAabb) L.flag |= uint32_t(t < prim_entry<D, N, kCast>(rec, L.r, L.pmin, L.pmax, L.fast));
               if (L.best_leaf == kNoHit || hit_before(t, id, L.best_t, L.best_leaf)) {
                 L.best_leaf = id;
                 L.best_t = t;
@@ -432,10 +508,13 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
     }
   };
 
+  bool pending = false;  // this lane's query waits to be answered again in reference order
   for (;;) {
-    // Refill the lanes without a query.
-    const bool need = !live && !exhausted;
+    // Refill the lanes without a query: a pending replay restarts its own
+    // query in the reference order, the others take the next ones.
+    const bool need = !live && !exhausted && !pending;
     const uint32_t need_mask = __ballot_sync(FULL, need);
+    uint32_t qs = kNoHit;
     if (need_mask) {
       const int leader = __ffs(need_mask) - 1;
       uint32_t base = 0;
@@ -443,15 +522,22 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
       base = __shfl_sync(FULL, base, leader);
       if (need) {
         const uint32_t q = base + uint32_t(__popc(need_mask & lt_mask));
-        if (q < p.n) {
-          live = start(q);
-          if (!live) finish();
-        } else {
-          exhausted = true;
-        }
+        if (q < n_queries) qs = q;
+        else exhausted = true;
       }
     }
-    const uint32_t live_mask = __ballot_sync(FULL, live);
+    bool replay = false;
+    if (pending) {
+      qs = L.q;
+      pending = false;
+      replay = true;
+    }
+    if (qs != kNoHit) {
+      L.ref = replay;
+      live = start(qs);
+      if (!live) finish();
+    }
+    const uint32_t live_mask = __ballot_sync(FULL, live || pending);
     if (!live_mask) {
       if (__all_sync(FULL, exhausted)) break;
       continue;
@@ -471,7 +557,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
         if (pa && pb) {
           // Reference order: child_a waits, child_b goes first. Near-first:
           // the smaller entry goes first.
-          const bool a_first = (REF || !kNearest) ? false : (ta <= tb);
+          const bool a_first = (REF || !kNearest) ? false : (!L.ref && ta <= tb);
           s_code[L.sp * kThreads + tid] = a_first ? cb : ca;
           s_t[L.sp * kThreads + tid] = a_first ? tb : ta;
           ++L.sp;
@@ -490,10 +576,20 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
         done = !pop();
       }
       if (done) {
-        finish();
         live = false;
+        if (DETECT && !L.ref && (L.flag != 0u || L.min_pruned <= near_limit(L.limit, p.window))) {
+          pending = true;  // answered again in reference order at the top of the loop
+          ++replays;
+        } else {
+          finish();
+        }
       }
     }
+  }
+  if (DETECT && p.replay_count) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) replays += __shfl_down_sync(FULL, replays, o);
+    if (lane == 0 && replays) atomicAdd(p.replay_count, replays);
   }
   if (STATS) {
 #pragma unroll
