@@ -221,6 +221,24 @@ int32_t sq_overlap(sq_ctx* ctx, const sq_bvh* bvh, const float* regions, uint32_
 int32_t sq_overlap_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_regions, uint32_t n, const sq_filter* filter,
                      uint64_t* d_offsets, uint32_t* d_leaves, uint64_t leaf_capacity, uint64_t* total);
 
+/* Overlap (as sq_overlap_d) without any device allocation. No counterpart in
+ * the reference. For callers that may not allocate device memory at query
+ * time -- an engine that owns a fixed device-memory budget and forbids
+ * driver allocations, a real-time loop that cannot take an allocation's
+ * latency, code with no sq_ctx to hold scratch -- it keeps its scratch (the
+ * per-region counts and work counters) in one static device array of the
+ * library, sized for at most 1,048,576 regions (about 4 MiB per GPU that
+ * loads the library, held until the process exits). n beyond that returns
+ * SQ_ERR_CAPACITY, as does a result larger than leaf_capacity (*total is then
+ * set). Device pointers; runs on `stream` (a cudaStream_t, NULL = the legacy
+ * default stream) and returns when the results are written. The first call
+ * on a device looks up the array's address on that device: make that first
+ * call before any stream capture. Every call shares the one array, so calls
+ * that overlap on the GPU (from several threads or streams) race. */
+int32_t sq_overlap_noalloc(const sq_bvh* bvh, const float* d_regions, uint32_t n, const sq_filter* filter,
+                           uint64_t* d_offsets, uint32_t* d_leaves, uint64_t leaf_capacity, uint64_t* total,
+                           void* stream);
+
 /* ---- two-level scenes (accel/tlas.rs) -------------------------------------
  * A Tlas over instances of one kind. Mesh instances (D = 3) reference a BLAS
  * of a shared BLAS set and carry a uniform scale: the instance's local test is

@@ -119,6 +119,7 @@ SIGNATURES = {
     "sq_shapecast_all_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, P, P, P]),
     "sq_overlap": (C.c_int32, [P, P, P, C.c_uint32, P, P, P, C.c_uint64, C.POINTER(C.c_uint64)]),
     "sq_overlap_d": (C.c_int32, [P, P, P, C.c_uint32, P, P, P, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "sq_overlap_noalloc": (C.c_int32, [P, P, C.c_uint32, P, P, P, C.c_uint64, C.POINTER(C.c_uint64), P]),
     "sq_blas_set_upload": (C.c_int32, [P, C.c_uint32, P, P, P, P, P, P, P, P, C.POINTER(P)]),
     "sq_blas_set_destroy": (C.c_int32, [P]),
     "sq_instance_world_aabbs": (C.c_int32, [C.c_int32, C.c_int32, C.c_uint32, P, P, P, P, P, P]),

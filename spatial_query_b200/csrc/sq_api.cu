@@ -792,3 +792,151 @@ extern "C" int32_t sq_overlap(sq_ctx* ctx, const sq_bvh* b, const float* regions
   if ((rc2 = finish(ctx))) return rc2;
   return rc;
 }
+
+// ============================================================================
+// Overlap without allocation.
+//
+// For callers that may not allocate device memory at query time: a host
+// engine that owns a fixed device-memory budget and forbids driver
+// allocations, a real-time loop where an allocation's latency is not
+// allowed, or code that has no context object to hold one. The scratch this
+// query needs -- per-region counts and the persistent kernels' work
+// counters -- lives in one file-scope device array, sized for at most
+// kNoAllocMaxRegions regions (about 4 MiB, held by every GPU that loads the
+// library until the process exits).
+// ============================================================================
+
+namespace {
+
+constexpr uint32_t kNoAllocMaxRegions = 1u << 20;
+constexpr uint32_t kNoAllocCounters = 2;  // work counters of the count and fill launches
+
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocMaxRegions + 1 + kNoAllocCounters];
+
+struct NoAllocDevice {
+  bool ready = false;
+  uint32_t* scratch = nullptr;  // device address of g_noalloc_scratch on this device
+  int sm_count = 0;
+  int blocks_per_sm = 1;
+};
+
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+// Exclusive prefix sum of n counts into offsets[0..n], offsets[n] = total, in
+// one block (n <= kNoAllocMaxRegions): each thread sums a contiguous run, the
+// block scans the run totals, each thread writes its run.
+__global__ void __launch_bounds__(1024) noalloc_scan_kernel(const uint32_t* counts, unsigned long long* offsets,
+                                                            uint32_t n) {
+  __shared__ unsigned long long part[1024];
+  const uint32_t t = threadIdx.x;
+  const uint32_t per = (n + 1023u) / 1024u;
+  const uint32_t lo = min(n, t * per), hi = min(n, lo + per);
+  unsigned long long s = 0;
+  for (uint32_t i = lo; i < hi; ++i) s += counts[i];
+  part[t] = s;
+  __syncthreads();
+  for (uint32_t off = 1; off < 1024; off <<= 1) {
+    const unsigned long long v = t >= off ? part[t - off] : 0ull;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  unsigned long long base = part[t] - s;  // exclusive
+  for (uint32_t i = lo; i < hi; ++i) {
+    offsets[i] = base;
+    base += counts[i];
+  }
+  if (t == 1023) offsets[n] = part[1023];
+}
+
+}  // namespace
+
+// The device address of the static scratch, looked up once per device (with
+// that device current) by the first call on it.
+static int32_t noalloc_setup(int device, const void* overlap_fn, NoAllocDevice** out) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return SQ_ERR_INVALID;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoAllocDevice& d = g_noalloc_dev[device];
+  if (!d.ready) {
+    if (cudaSetDevice(device) != cudaSuccess) return SQ_ERR_CUDA;
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) {
+      cudaGetLastError();
+      return SQ_ERR_CUDA;
+    }
+    int sms = 0, bps = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return SQ_ERR_CUDA;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, overlap_fn, kThreads, 0) != cudaSuccess || bps < 1) bps = 1;
+    d.scratch = static_cast<uint32_t*>(ptr);
+    d.sm_count = sms;
+    d.blocks_per_sm = bps;
+    d.ready = true;
+  }
+  *out = &d;
+  return SQ_OK;
+}
+
+extern "C" int32_t sq_overlap_noalloc(const sq_bvh* b, const float* d_regions, uint32_t n, const sq_filter* f,
+                                      uint64_t* d_offsets, uint32_t* d_leaves, uint64_t leaf_capacity,
+                                      uint64_t* total, void* stream) {
+  if (!b || !d_offsets || !total || (n && !d_regions)) return SQ_ERR_INVALID;
+  if (n > kNoAllocMaxRegions) return SQ_ERR_CAPACITY;  // beyond the static scratch
+  NoAllocDevice* d = nullptr;
+  int32_t rc = noalloc_setup(b->device, b->ks.overlap, &d);
+  if (rc) return rc;
+  if (cudaSetDevice(b->device) != cudaSuccess) return SQ_ERR_CUDA;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  uint32_t* counts = d->scratch;
+  uint32_t* counters = d->scratch + kNoAllocMaxRegions + 1;
+  // Every call shares the scratch: the counts and both work counters start at zero.
+  if (cudaMemsetAsync(counts, 0, (size_t(n) + 1) * sizeof(uint32_t), s) != cudaSuccess ||
+      cudaMemsetAsync(counters, 0, kNoAllocCounters * sizeof(uint32_t), s) != cudaSuccess)
+    return SQ_ERR_CUDA;
+  const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(d->sm_count) * d->blocks_per_sm,
+                                                                  (uint64_t(n) + kThreads - 1) / kThreads));
+  const int stack = int(std::max<uint32_t>(b->depth, 1));
+  const size_t smem = size_t(stack) * kThreads * 8;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(b->ks.overlap, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+    return SQ_ERR_CUDA;
+  if (b->n_nodes != 0 && n != 0) {
+    QueryParams p;
+    base_params(b, f, p);
+    p.queries = d_regions;
+    p.n = n;
+    p.out_count = counts;
+    p.fill = 0;
+    p.counter = counters;
+    p.stack = stack;
+    void* args[] = {&p};
+    if (cudaLaunchKernel(b->ks.overlap, dim3(unsigned(grid)), dim3(kThreads), args, smem, s) != cudaSuccess)
+      return SQ_ERR_CUDA;
+  }
+  noalloc_scan_kernel<<<1, 1024, 0, s>>>(counts, reinterpret_cast<unsigned long long*>(d_offsets), n);
+  unsigned long long tot = 0;
+  if (cudaMemcpyAsync(&tot, d_offsets + n, sizeof(tot), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return SQ_ERR_CUDA;
+  *total = tot;
+  if (tot > leaf_capacity) return SQ_ERR_CAPACITY;
+  if (tot && b->n_nodes != 0) {
+    if (!d_leaves) return SQ_ERR_INVALID;
+    QueryParams p;
+    base_params(b, f, p);
+    p.queries = d_regions;
+    p.n = n;
+    p.out_count = counts;
+    p.fill = 1;
+    p.csr_offsets = reinterpret_cast<const unsigned long long*>(d_offsets);
+    p.csr_leaves = d_leaves;
+    p.counter = counters + 1;
+    p.stack = stack;
+    void* args[] = {&p};
+    if (cudaLaunchKernel(b->ks.overlap, dim3(unsigned(grid)), dim3(kThreads), args, smem, s) != cudaSuccess)
+      return SQ_ERR_CUDA;
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return SQ_ERR_CUDA;
+  return SQ_OK;
+}

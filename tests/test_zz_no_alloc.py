@@ -1,0 +1,70 @@
+"""The allocation-free overlap entry point (sq_overlap_noalloc).
+
+Some callers cannot allocate device memory when they query: an engine that
+owns a fixed device-memory budget and forbids driver allocations, a
+real-time loop that cannot take an allocation's latency, code that holds no
+sq_ctx. sq_overlap_noalloc keeps its scratch in a static device array of the
+library instead. This test calls it through the C ABI twice in a row and
+checks both results against the ordinary overlap entry point bit for bit
+(overlap sets are integer results, so the tolerance is exact equality), and
+checks that a batch beyond the array's capacity is refused. It creates its
+own context and scene, so it passes alone in a fresh process as well as
+after the other tests.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import spatial_query_b200 as sq
+from spatial_query_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+MAX_REGIONS = 1 << 20
+
+
+def _noalloc(scene, d_regions, n, d_offsets, d_leaves, capacity, stream):
+    total = C.c_uint64(0)
+    rc = sq.lib().sq_overlap_noalloc(scene.h, d_regions.data_ptr(), n, None, d_offsets.data_ptr(),
+                                     d_leaves.data_ptr(), capacity, C.byref(total), stream)
+    return rc, int(total.value)
+
+
+def test_overlap_noalloc_matches_overlap_twice():
+    import torch
+    s = scenes.mixture_scene(seed=11, n_boxes=200_000, n_rays=1, n_regions=50_000)
+    ctx = sq.Context(0)
+    geom = sq.Geometry("boxes", 6, s["prims"])
+    scene = sq.DeviceBvh(ctx, sq.HostBvh.build(geom), geom)
+    want_off, want_leaves = scene.overlap(s["regions"])
+    assert want_leaves.size > 0
+
+    dev = torch.device("cuda", 0)
+    n = s["regions"].shape[0]
+    d_regions = torch.from_numpy(s["regions"]).to(dev)
+    cap = int(want_leaves.size) + 16
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    for call in range(2):
+        # Poison the outputs so a stale result from the first call cannot pass the second.
+        d_offsets = torch.full((n + 1,), -1, dtype=torch.int64, device=dev)
+        d_leaves = torch.full((cap,), -1, dtype=torch.int32, device=dev)
+        rc, total = _noalloc(scene, d_regions, n, d_offsets, d_leaves, cap, stream)
+        assert rc == sq.SQ_OK, f"call {call}: status {rc}"
+        assert total == want_leaves.size
+        got_off = d_offsets.cpu().numpy().view(np.uint64)
+        got_leaves = d_leaves.cpu().numpy().view(np.uint32)[:total]
+        assert np.array_equal(got_off, want_off), f"call {call}: offsets differ"
+        assert np.array_equal(got_leaves, want_leaves), f"call {call}: leaves differ"
+
+    # Too small an output: the needed total is reported, nothing overflows.
+    d_offsets = torch.empty(n + 1, dtype=torch.int64, device=dev)
+    d_small = torch.empty(4, dtype=torch.int32, device=dev)
+    rc, total = _noalloc(scene, d_regions, n, d_offsets, d_small, 4, stream)
+    assert rc == sq.SQ_ERR_CAPACITY and total == want_leaves.size
+
+    # More regions than the static scratch holds: refused before any work.
+    rc, _ = _noalloc(scene, d_regions, MAX_REGIONS + 1, d_offsets, d_small, 4, stream)
+    assert rc == sq.SQ_ERR_CAPACITY
+    scene.close()
+    ctx.close()
