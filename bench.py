@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--order", default="reference", choices=["near_first", "reference"])
+    ap.add_argument("--order", default="near_first", choices=["near_first", "reference"])
     ap.add_argument("--rays", type=int, default=1 << 20,
                     help="rays per step (half coherent, half incoherent); the metric is quoted at 1,048,576")
     return ap.parse_args()

@@ -56,10 +56,11 @@ extern "C" {
 #define SQ_NARROW_TRIANGLE 3    /* leaf = v0,v1,v2 (D = 3); Moeller-Trumbore (viewport-lib-query/src/lib.rs:295-320) */
 
 /* Traversal order of nearest queries (sq_ctx_set_order). */
-#define SQ_ORDER_NEAR_FIRST 0   /* visit the child with the smaller slab entry first; a query whose answer
-                                   could depend on the order is answered again in the reference order */
-#define SQ_ORDER_REFERENCE 1    /* the default: the crate's own order (accel/bvh.rs:119-120), replaying
-                                   the CPU's decisions step for step */
+#define SQ_ORDER_NEAR_FIRST 0   /* the default: visit the child with the smaller slab entry first; an answer
+                                   that is not certified order-independent is recomputed in the reference
+                                   order by a second launch */
+#define SQ_ORDER_REFERENCE 1    /* the crate's own order (accel/bvh.rs:119-120), replaying the CPU's
+                                   decisions step for step (QueryStats counters included) */
 
 typedef struct sq_ctx sq_ctx;
 typedef struct sq_bvh sq_bvh;
@@ -126,14 +127,15 @@ const char* sq_ctx_last_error(const sq_ctx* ctx);
 void* sq_ctx_stream(sq_ctx* ctx);
 int32_t sq_ctx_set_stream(sq_ctx* ctx, void* stream);
 int32_t sq_ctx_synchronize(sq_ctx* ctx);
-/* Nearest-query order (SQ_ORDER_*, default SQ_ORDER_REFERENCE) and
+/* Nearest-query order (SQ_ORDER_*, default SQ_ORDER_NEAR_FIRST) and
  * persistent-grid blocks per SM (0 = occupancy). */
 int32_t sq_ctx_set_order(sq_ctx* ctx, int32_t order);
 int32_t sq_ctx_set_blocks_per_sm(sq_ctx* ctx, int32_t blocks);
-/* Near-first nearest queries are answered again in the reference order when
- * their answer could depend on the visiting order: when a hit lies before
- * its primitive's own AABB entry, or when a node pruned by the limit had its
- * entry within `window` (relative, default 2^-16) past the final limit. */
+/* Near-first nearest queries prune a node only when its slab entry lies more
+ * than `window` (relative, default 2^-16) past the current limit, and are
+ * answered again in the reference order when their answer comes before the
+ * slab entry of its own primitive's AABB (the one case where the reference's
+ * walk could miss it). */
 int32_t sq_ctx_set_replay_window(sq_ctx* ctx, float window);
 /* Kernels this context has launched so far. */
 uint64_t sq_ctx_launch_count(const sq_ctx* ctx);

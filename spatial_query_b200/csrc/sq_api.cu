@@ -24,29 +24,6 @@
 #include "sq_internal.cuh"
 
 using namespace sq;
-struct sq_bvh {
-  int device = 0;
-  int dim = 0;
-  int narrow = 0;
-  uint32_t n_nodes = 0, n_prims = 0, n_interior = 0, depth = 0, n_leaves = 0;
-  uint32_t stride = 0;
-  uint32_t root_code = 0;
-  float4* d_nodes = nullptr;
-  float4* d_prims = nullptr;
-  float* d_root = nullptr;
-  uint64_t* d_layers = nullptr;
-  uint32_t* d_sub = nullptr;
-  uint32_t* d_prim_ids = nullptr;
-  RefitLeaf* d_leaves = nullptr;
-  uint32_t* d_parents = nullptr;
-  uint32_t* d_arrivals = nullptr;
-  float* d_refit_in = nullptr;  // staging for host refit data
-  int* d_nonfinite = nullptr;   // non-zero when some node bound is not finite
-  KernelSet ks{};
-  size_t bytes = 0;
-  std::vector<uint32_t> h_iidx;  // host node -> interior record (or kNoHit)
-  std::vector<uint32_t> h_child_a, h_child_b, h_count;
-};
 
 namespace {
 
@@ -105,11 +82,8 @@ int32_t nearest_core(sq_ctx* ctx, const sq_bvh* b, bool cast, const float* d_q, 
   if (stats && !cast) p.stats = ctx->d_stats;
   const void* ref_fn = cast ? b->ks.cast_nearest[1] : b->ks.ray_nearest[1][st];
   if (!near_first) return launch_persistent(ctx, ref_fn, p, b->depth, p.n);
-  CK(cudaMemsetAsync(ctx->d_replays, 0, sizeof(uint32_t), ctx->stream));
-  p.replay_count = ctx->d_replays;
-  p.window = ctx->window;
   const void* near_fn = cast ? b->ks.cast_nearest[0] : b->ks.ray_nearest[0][st];
-  return launch_persistent(ctx, near_fn, p, b->depth, p.n);
+  return near_first_launch(ctx, b, near_fn, ref_fn, p, b->depth);
 }
 
 int32_t list_core(sq_ctx* ctx, const sq_bvh* b, int kind, const float* d_q, uint32_t n, float max_toi,
@@ -214,6 +188,7 @@ extern "C" int32_t sq_ctx_destroy(sq_ctx* ctx) {
   if (ctx->own) cudaStreamSynchronize(ctx->own);
   if (ctx->arena.p) cudaFree(ctx->arena.p);
   if (ctx->d_replays) cudaFree(ctx->d_replays);
+  if (ctx->replay_list.p) cudaFree(ctx->replay_list.p);
   if (ctx->d_counters) cudaFree(ctx->d_counters);
   if (ctx->d_stats) cudaFree(ctx->d_stats);
   if (ctx->own) cudaStreamDestroy(ctx->own);
@@ -939,4 +914,72 @@ extern "C" int32_t sq_overlap_noalloc(const sq_bvh* b, const float* d_regions, u
   }
   if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return SQ_ERR_CUDA;
   return SQ_OK;
+}
+
+// ============================================================================
+// learned-seeded nearest rays (the learned guide's query, include/sq_guide.h)
+// ============================================================================
+
+int32_t sqi::seeded_nearest(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, uint32_t n, float max_toi,
+                            const int32_t* d_bucket, const uint2* d_buckets, uint32_t n_buckets, const sq_hits& o,
+                            sq_query_stats* st) {
+  int32_t rc = check_scene(ctx, b);
+  if (rc) return rc;
+  if (!o.leaf || (n && (!d_rays || !d_bucket))) return fail(ctx, SQ_ERR_INVALID, "null argument");
+  if (!b->ks.ray_nearest_seeded[0]) return fail(ctx, SQ_ERR_UNSUPPORTED, "seeded queries need a D = 3 scene");
+  if ((rc = stats_begin(ctx, st))) return rc;
+  if (n && b->n_nodes == 0) {
+    if ((rc = nearest_core(ctx, b, false, d_rays, n, max_toi, nullptr, nullptr, o, false))) return rc;
+  } else if (n) {
+    QueryParams p;
+    base_params(b, nullptr, p);
+    p.queries = d_rays;
+    p.max_toi = max_toi;
+    p.n = n;
+    p.out_leaf = o.leaf;
+    p.out_toi = o.toi;
+    p.out_sub = o.sub_object;
+    p.out_normal = o.normal;
+    p.out_point = o.point;
+    p.seed_bucket = d_bucket;
+    p.buckets = d_buckets;
+    p.n_buckets = n_buckets;
+    if (st) p.stats = ctx->d_stats;
+    // one stack entry more than the depth: the root waits below the bucket
+    if ((rc = near_first_launch(ctx, b, b->ks.ray_nearest_seeded[st ? 1 : 0], b->ks.ray_nearest[1][st ? 1 : 0], p,
+                                b->depth + 1)))
+      return rc;
+  }
+  if ((rc = finish(ctx))) return rc;
+  return stats_end(ctx, st);
+}
+
+int32_t sqi::near_first_launch(sq_ctx* ctx, const sq_bvh* b, const void* fn, const void* ref_fn, QueryParams& p,
+                               uint32_t stack) {
+  (void)b;
+  // The replay list holds at most every query of the batch; it grows here,
+  // outside any stream capture once a batch of this size has run.
+  const size_t need = size_t(std::max<uint32_t>(p.n, 1)) * sizeof(uint32_t);
+  if (ctx->replay_list.cap < need) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->replay_list.p) CK(cudaFree(ctx->replay_list.p));
+    ctx->replay_list.p = nullptr;
+    ctx->replay_list.cap = 0;
+    CK(cudaMalloc(&ctx->replay_list.p, need));
+    ctx->replay_list.cap = need;
+  }
+  CK(cudaMemsetAsync(ctx->d_replays, 0, sizeof(uint32_t), ctx->stream));
+  p.replay_count = ctx->d_replays;
+  p.replay_list = static_cast<uint32_t*>(ctx->replay_list.p);
+  p.window = ctx->window;
+  int32_t rc = launch_persistent(ctx, fn, p, stack, p.n);
+  if (rc) return rc;
+  // The uncertified queries again, in the reference order, unseeded.
+  QueryParams r = p;
+  r.replay_count = nullptr;
+  r.replay_list = nullptr;
+  r.seed_bucket = nullptr;
+  r.q_list = static_cast<const uint32_t*>(ctx->replay_list.p);
+  r.q_count = ctx->d_replays;
+  return launch_persistent(ctx, ref_fn, r, b->depth, p.n);
 }

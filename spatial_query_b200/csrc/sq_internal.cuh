@@ -39,21 +39,58 @@ struct sq_ctx {
   cudaStream_t stream = nullptr;
   std::string err;
   int sm_count = 0;
-  int order = SQ_ORDER_REFERENCE;  // exact by construction; near-first is opt-in
+  int order = SQ_ORDER_NEAR_FIRST;  // certified near-first; the reference order on request
   int blocks_per_sm = 0;
   uint32_t* d_counters = nullptr;
   uint32_t slot = 0;
   unsigned long long* d_stats = nullptr;
   sqi::DevBuf arena;
   uint32_t* d_replays = nullptr;  // queries of the last near-first launch answered again in reference order
-  float window = 0x1p-16f;        // relative window past the limit that flags a pruned node
+  sqi::DevBuf replay_list;        // their indices (grown to the largest batch)
+  float window = 0x1p-16f;        // relative window past the limit within which near-first still visits nodes
   uint64_t launches = 0;
   std::unordered_map<uint64_t, int> occ;  // (kernel, dynamic smem) -> resident blocks per SM
+};
+
+// An uploaded scene: device records plus the host topology (kept for the
+// learned guide's bucket table and for reading bounds back).
+struct sq_bvh {
+  int device = 0;
+  int dim = 0;
+  int narrow = 0;
+  uint32_t n_nodes = 0, n_prims = 0, n_interior = 0, depth = 0, n_leaves = 0;
+  uint32_t stride = 0;
+  uint32_t root_code = 0;
+  float4* d_nodes = nullptr;
+  float4* d_prims = nullptr;
+  float* d_root = nullptr;
+  uint64_t* d_layers = nullptr;
+  uint32_t* d_sub = nullptr;
+  uint32_t* d_prim_ids = nullptr;
+  sq::RefitLeaf* d_leaves = nullptr;
+  uint32_t* d_parents = nullptr;
+  uint32_t* d_arrivals = nullptr;
+  float* d_refit_in = nullptr;  // staging for host refit data
+  int* d_nonfinite = nullptr;   // non-zero when some node bound is not finite
+  sq::KernelSet ks{};
+  size_t bytes = 0;
+  std::vector<uint32_t> h_iidx;  // host node -> interior record (or kNoHit)
+  std::vector<uint32_t> h_child_a, h_child_b, h_count;
 };
 
 namespace sqi {
 
 using namespace sq;
+
+// Near-first nearest launch `fn` followed by the reference-order replay of
+// the queries it could not certify (sq_api.cu).
+int32_t near_first_launch(sq_ctx* ctx, const sq_bvh* b, const void* fn, const void* ref_fn, QueryParams& p,
+                          uint32_t stack);
+
+// Learned-seeded nearest rays (sq_api.cu): enqueues the SEED kernel.
+int32_t seeded_nearest(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, uint32_t n, float max_toi,
+                       const int32_t* d_bucket, const uint2* d_buckets, uint32_t n_buckets, const sq_hits& o,
+                       sq_query_stats* st);
 
 inline int32_t fail(sq_ctx* c, int32_t code, const std::string& msg) {
   if (c) c->err = msg;

@@ -98,7 +98,7 @@ struct TlasParams {
   int stack;
   int blas_finite;  // every BLAS bound is finite
   uint32_t* replay_count;  // optional: queries answered again in the reference order
-  float window;            // relative window past the limit that flags a pruned node
+  float window;            // relative window past the limit within which near-first still visits nodes
 };
 
 __device__ __forceinline__ bool t_accepts(const TlasParams& p, uint32_t id) {
@@ -186,23 +186,16 @@ __device__ __forceinline__ bool blas_nearest(const TlasParams& p, uint32_t b, co
                                              bool ref) {
   const BlasRoot R = p.broots[b];
   float limit = mt;
+  float cut = mt;  // near-first prunes past a small window beyond the limit (traverse.cuh)
   const float kInf = __int_as_float(0x7f800000);
-  float min_pruned = kInf;
-  // The slab without the limit, then the entry against the limit; the
-  // smallest entry pruned by the limit decides the near-first flag at the end
-  // (traverse.cuh).
+  // The slab without the limit, then the entry against the cut.
   auto test = [&](const float* lo, const float* hi, float& te) -> bool {
     int ax;
     const bool geo = fast ? slab_fast<3>(r, lo, hi, kInf, te) : slab<3>(r, lo, hi, kInf, te, ax);
-    const bool pass = geo && te <= limit;
-    if (!REF) min_pruned = fminf(min_pruned, (geo && !pass) ? te : kInf);
-    return pass;
+    return geo && te <= cut;
   };
   float te0;
-  if (!test(R.lo, R.hi, te0)) {
-    if (!REF) flag |= uint32_t(min_pruned <= near_limit(limit, p.window));
-    return false;
-  }
+  if (!test(R.lo, R.hi, te0)) return false;
   uint32_t code = R.code;
   int sp = base;
   uint32_t best = kNoHit;
@@ -233,8 +226,7 @@ __device__ __forceinline__ bool blas_nearest(const TlasParams& p, uint32_t b, co
           --sp;
           code = s_code[sp * kThreads + tid];
           const float t = s_t[sp * kThreads + tid];
-          if (t <= limit) { found = true; break; }
-          if (!REF) min_pruned = fminf(min_pruned, t);
+          if (t <= cut) { found = true; break; }
         }
         if (!found) { done = true; break; }
       }
@@ -248,19 +240,22 @@ __device__ __forceinline__ bool blas_nearest(const TlasParams& p, uint32_t b, co
       const uint32_t id = idw & ~kLeafBit;
       float t, nrm[3];
       if (ray_triangle(r.o, r.d, rec, rec + 3, rec + 6, t) && !(t > limit)) {
-        if (!REF) {
-          float lo[3], hi[3], te;
-          int ax;
-          tri_aabb(rec, rec + 3, rec + 6, lo, hi);
-          if (fast) slab_fast<3>(r, lo, hi, kInf, te);
-          else slab<3>(r, lo, hi, kInf, te, ax);
-          flag |= uint32_t(t < te);
-        }
         if (best == kNoHit || hit_before(t, id, best_t, best)) {
           tri_normal(rec, rec + 3, rec + 6, nrm);
           best = id;
           best_t = t;
           limit = t;
+          cut = t;
+          if (!REF && !ref) {
+            // certify the new best: not before its own triangle's AABB entry
+            float lo[3], hi[3], te;
+            int ax;
+            tri_aabb(rec, rec + 3, rec + 6, lo, hi);
+            if (fast) slab_fast<3>(r, lo, hi, kInf, te);
+            else slab<3>(r, lo, hi, kInf, te, ax);
+            flag = uint32_t(t < te);
+            cut = near_limit(t, p.window);
+          }
           best_n[0] = nrm[0];
           best_n[1] = nrm[1];
           best_n[2] = nrm[2];
@@ -274,12 +269,10 @@ __device__ __forceinline__ bool blas_nearest(const TlasParams& p, uint32_t b, co
       --sp;
       code = s_code[sp * kThreads + tid];
       const float t = s_t[sp * kThreads + tid];
-      if (t <= limit) { found = true; break; }
-      if (!REF) min_pruned = fminf(min_pruned, t);
+      if (t <= cut) { found = true; break; }
     }
     if (!found) break;
   }
-  if (!REF) flag |= uint32_t(min_pruned <= near_limit(limit, p.window));
   if (best == kNoHit) return false;
   t_out = best_t;
   leaf_out = best;
@@ -293,8 +286,8 @@ template <int D> struct TLane {
   RayPre<D> r;  // world ray or cast path; regions keep lo in o and hi in d
   float pmin[D], pmax[D];
   float limit;
-  float min_pruned;  // smallest entry among nodes pruned by the limit
-  uint32_t flag;     // a hit came before its own box's entry
+  float cut;         // nodes whose entry lies past this are pruned
+  uint32_t flag;     // the best hit so far is not certified (traverse.cuh)
   bool ref;          // this pass runs in the reference order (a replay)
   uint32_t q;
   int kind;
@@ -347,9 +340,7 @@ __global__ void __launch_bounds__(kThreads) tlas_kernel(const TlasParams p) {
     } else {
       geo = L.fast ? slab_fast<D>(L.r, lo, hi, kInf, te) : slab<D>(L.r, lo, hi, kInf, te, ax);
     }
-    const bool pass = geo && te <= L.limit;
-    if (!REF) L.min_pruned = fminf(L.min_pruned, (is_nearest() && geo && !pass) ? te : kInf);
-    return pass;
+    return geo && te <= L.cut;
   };
 
   auto pop = [&]() -> bool {
@@ -358,15 +349,13 @@ __global__ void __launch_bounds__(kThreads) tlas_kernel(const TlasParams p) {
       --L.sp;
       L.code = s_code[L.sp * kThreads + tid];
       const float t = s_t[L.sp * kThreads + tid];
-      if (!nearest || t <= L.limit) return true;
-      if (!REF) L.min_pruned = fminf(L.min_pruned, t);
+      if (!nearest || t <= L.cut) return true;
     }
     return false;
   };
 
   auto start = [&](uint32_t g) -> bool {
     L.flag = 0u;
-    L.min_pruned = kInf;
     const float* src;
     if (g < p.n_ray) {
       L.kind = p.ray_kind;
@@ -420,6 +409,7 @@ __global__ void __launch_bounds__(kThreads) tlas_kernel(const TlasParams p) {
     L.v_hit = 0;
     L.sp = 0;
     L.code = p.root_code;
+    L.cut = L.limit;
     float lo[D], hi[D];
 #pragma unroll
     for (int i = 0; i < D; ++i) {
@@ -486,14 +476,19 @@ __global__ void __launch_bounds__(kThreads) tlas_kernel(const TlasParams p) {
     return te;
   };
 
-  auto take = [&](float t, uint32_t id, uint32_t subv, const float* n, uint32_t pos) {
+  // `inner` is set when the instance's own nearest hit is not certified.
+  auto take = [&](float t, uint32_t id, uint32_t subv, const float* n, uint32_t pos, uint32_t inner) {
     if (is_nearest()) {
-      if (!REF) L.flag |= uint32_t(t < inst_entry(pos));
       if (L.best_leaf == kNoHit || hit_before(t, id, L.best_t, L.best_leaf)) {
         L.best_leaf = id;
         L.best_sub = subv;
         L.best_t = t;
         L.limit = t;
+        L.cut = t;
+        if (!REF && !L.ref) {
+          L.flag = inner | uint32_t(t < inst_entry(pos));
+          L.cut = near_limit(t, p.window);
+        }
 #pragma unroll
         for (int i = 0; i < D; ++i) L.best_n[i] = n[i];
       }
@@ -567,7 +562,7 @@ __global__ void __launch_bounds__(kThreads) tlas_kernel(const TlasParams p) {
           } else if constexpr (IK == kInstBall) {
             hit = ray_ball<D, true>(L.r.o, L.r.d, tr, fadd(rec[IL::param], L.pmax[0]), L.limit, t, n);
           }
-          if (hit) take(t, id, IK == kInstMesh ? kNoHit : subv, n, pos);
+          if (hit) take(t, id, IK == kInstMesh ? kNoHit : subv, n, pos, 0u);
         } else {
           if (STATS) L.v_nar += 1;
           // World ray -> instance space (tlas.rs:465-471).
@@ -594,14 +589,13 @@ __global__ void __launch_bounds__(kThreads) tlas_kernel(const TlasParams p) {
             uint32_t bflag = 0u;
             const bool bh = blas_nearest<REF>(p, __float_as_uint(rec[IL::blas]), lr, f && !isnan(mts), mts, s_code,
                                               s_t, tid, L.sp, ts, face, nl, bflag, L.ref);
-            L.flag |= bflag;  // the mesh's own nearest hit may depend on order
             if (bh) {
               const float toi = fmul(ts, s);
               if (!(toi > L.limit)) {
                 float nw[3];
                 rotate<3>(R, nl, nw);
                 if (STATS) L.v_hit += 1;
-                take(toi, id, face, nw, pos);
+                take(toi, id, face, nw, pos, bflag);
               }
             }
           } else if constexpr (IK == kInstBox) {
@@ -609,7 +603,7 @@ __global__ void __launch_bounds__(kThreads) tlas_kernel(const TlasParams p) {
             if (ray_local_box<D>(lo, ld, rec + IL::param, L.limit, t, nl)) {
               rotate<D>(R, nl, nw);
               if (STATS) L.v_hit += 1;
-              take(t, id, subv, nw, pos);
+              take(t, id, subv, nw, pos, 0u);
             }
           } else {
             const float rr = rec[IL::param];
@@ -629,7 +623,7 @@ __global__ void __launch_bounds__(kThreads) tlas_kernel(const TlasParams p) {
                     normalize_or_zero<D>(nl);
                     rotate<D>(R, nl, nw);
                     if (STATS) L.v_hit += 1;
-                    take(tt, id, subv, nw, pos);
+                    take(tt, id, subv, nw, pos, 0u);
                   }
                 }
               }
@@ -640,7 +634,7 @@ __global__ void __launch_bounds__(kThreads) tlas_kernel(const TlasParams p) {
               if (ray_ball<D, true>(lo, ld, zero, rr, L.limit, t, nl)) {
                 rotate<D>(R, nl, nw);
                 if (STATS) L.v_hit += 1;
-                take(t, id, subv, nw, pos);
+                take(t, id, subv, nw, pos, 0u);
               }
             }
           }
@@ -715,7 +709,7 @@ __global__ void __launch_bounds__(kThreads) tlas_kernel(const TlasParams p) {
       }
       if (done) {
         live = false;
-        if (!REF && !L.ref && (L.flag != 0u || L.min_pruned <= near_limit(L.limit, p.window))) {
+        if (!REF && !L.ref && L.flag != 0u) {
           // answered again in the reference order at the top of the loop
           pending = true;
           pending_g = L.q + (L.kind <= kTRayCross ? 0u : (L.kind <= kTCastAll ? p.n_ray : p.n_ray + p.n_cast));

@@ -63,11 +63,17 @@ struct QueryParams {
   uint32_t* csr_leaves;
   unsigned long long* stats;
   uint32_t* query_stats;  // optional per-query counters [n][4] (u32)
-  uint32_t* replay_count;  // optional: queries answered again in the reference order
-  float window;            // relative window past the limit that flags a pruned node
+  uint32_t* replay_count;  // near-first: number of uncertified queries appended to replay_list
+  uint32_t* replay_list;   // near-first: their indices
+  const uint32_t* q_list;  // optional: work item i is query q_list[i] ...
+  const uint32_t* q_count; // ... for i < *q_count (the reference-order replay of replay_list)
+  float window;            // relative window past the limit within which near-first still visits nodes
   unsigned long long mask;
   long long exclude;
   const float* root_box;  // min[D], max[D] of the root (device memory: refit updates it)
+  const int32_t* seed_bucket;  // learned guide: predicted bucket per query (seeded launches)
+  const uint2* buckets;        // per bucket: node code, parent record << 1 | slot (kNoHit: the root)
+  uint32_t n_buckets;
   const int* nonfinite;   // non-zero when some node bound is not finite (device memory)
   float max_toi;
   int stack;              // traversal-stack entries per thread (dynamic shared memory)
@@ -95,15 +101,17 @@ template <int NV> __device__ __forceinline__ void load_vec(const float4* __restr
   }
 }
 
-// Near-first traversal visits nodes in another order than the reference. The
-// answers agree unless a primitive's hit rounds to before the slab entry of
-// its own leaf (possible for balls and triangles by a few ulps) and another
-// hit lies in between. A lane flags its query when it sees such a hit, or
-// when some node it pruned by the limit has an entry within a small relative
-// window (2^-16 by default) past the final limit (where an unseen primitive of that kind could
-// hide a hit no later than the answer; later hits cannot change it). A
-// flagged query is answered again at once, by the same lane, in the
-// reference order.
+// Near-first traversal visits nodes in another order than the reference, so
+// its answer is certified before it counts. The reference's limit never
+// drops below the global minimum hit h, and every box enclosing h's
+// primitive has a slab entry no later than the entry of the primitive's own
+// AABB; so when h.toi is not before that entry, the reference's walk reaches
+// h whatever its order and answers h. Near-first prunes a node only when its
+// entry lies past the best hit by more than a small relative window (2^-16 by
+// default), which finds h whenever no hit is computed that far before the
+// entry of a box enclosing its primitive. A query whose answer comes before
+// its own primitive's AABB entry is not certified: it is appended to a list
+// that a second launch answers again in the reference order.
 __device__ __forceinline__ float near_limit(float limit, float window) {
   return __fadd_rn(limit, __fadd_rn(__fmul_rn(fabsf(limit), window), 0x1p-20f));
 }
@@ -248,12 +256,11 @@ __device__ __forceinline__ void list_insert(const QueryParams& p, uint32_t q, ui
 template <int D, int K> struct Lane {
   RayPre<D> r;
   float pmin[D], pmax[D];
-  float limit;
-  float min_pruned;  // smallest entry among nodes pruned by the limit
-  uint32_t flag;     // a hit came before its own primitive's AABB entry
-  bool ref;          // this pass runs in the reference order (a replay)
+  float limit;       // nodes whose entry lies past this are pruned (near-first: the best hit plus the window)
+  uint32_t best_pos; // near-first: primitive position of the best hit (for its certification)
   uint32_t q;
   uint32_t code;
+  uint32_t skip;     // seeded: the bucket subtree already searched first
   int sp;
   bool fast;
   uint32_t best_leaf;
@@ -270,7 +277,12 @@ template <int D, int K> struct Lane {
 // slowest query. Between refills a lane descends interior records until it
 // reaches a leaf, tests that leaf's primitives and pops the next waiting
 // child (Aila and Laine's while-while loop with dynamic fetch).
-template <int D, int N, int K, bool REF, bool STATS>
+//
+// SEED (nearest rays only): the learned guide's predicted bucket, a subtree
+// at a fixed depth, is searched first; its nearest hit becomes the limit
+// for the rest of the walk from the root, which skips that subtree. The
+// answer is certified exactly as in near-first, so it is the reference's.
+template <int D, int N, int K, bool REF, bool STATS, bool SEED = false>
 __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   constexpr bool kNearest = (K == kRayNearest || K == kCastNearest);
   constexpr bool kCast = (K == kCastNearest || K == kCastAll);
@@ -292,8 +304,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   unsigned long long c_vis = 0, c_nar = 0, c_hit = 0;
   Lane<D, K> L;
   bool live = false, exhausted = false;
-  const uint32_t n_queries = p.n;
-  uint32_t replays = 0;
+  const uint32_t n_queries = p.q_count ? *p.q_count : p.n;
 
   constexpr bool DETECT = kNearest && !REF;
   const float kInf = __int_as_float(0x7f800000);
@@ -314,9 +325,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
       } else {
         geo = L.fast ? slab_fast<D>(L.r, lo, hi, kInf, te) : slab<D>(L.r, lo, hi, kInf, te, ax);
       }
-      const bool pass = geo && te <= L.limit;
-      if (DETECT) L.min_pruned = fminf(L.min_pruned, (geo && !pass) ? te : kInf);
-      return pass;
+      return geo && te <= L.limit;
     }
   };
 
@@ -328,13 +337,21 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
       L.code = s_code[L.sp * kThreads + tid];
       const float t = s_t[L.sp * kThreads + tid];
       if (!kNearest || t <= L.limit) return true;
-      if (DETECT) L.min_pruned = fminf(L.min_pruned, t);
     }
     return false;
   };
 
   auto finish = [&]() {
     const uint32_t q = L.q;
+    if constexpr (DETECT && N != kNarrowAabb) {
+      // Certify the answer: not before its own primitive's AABB entry.
+      if (L.best_leaf != kNoHit) {
+        float rec[PL::vec * 4];
+        load_vec<PL::vec>(p.prims + size_t(L.best_pos) * PL::vec, rec);
+        if (L.best_t < prim_entry<D, N, kCast>(rec, L.r, L.pmin, L.pmax, L.fast))
+          p.replay_list[atomicAdd(p.replay_count, 1u)] = q;
+      }
+    }
     if constexpr (kNearest) {
       p.out_leaf[q] = L.best_leaf;
       if (p.out_toi) p.out_toi[q] = L.best_t;
@@ -375,8 +392,6 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   // Loads query q and tests the root. False when the query is already done.
   auto start = [&](uint32_t q) -> bool {
     L.q = q;
-    L.flag = 0u;
-    L.min_pruned = kInf;
     const float* src = p.queries + size_t(q) * QW;
 #pragma unroll
     for (int i = 0; i < D; ++i) {
@@ -421,7 +436,35 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
       hi[i] = p.root_box[D + i];
     }
     float te;
-    return test_box(lo, hi, te);
+    L.skip = kNoHit;
+    const bool hit_root = test_box(lo, hi, te);
+    if constexpr (SEED) {
+      const int32_t bk = p.seed_bucket[q];
+      if (hit_root && bk >= 0 && uint32_t(bk) < p.n_buckets) {
+        const uint2 e = __ldg(p.buckets + bk);
+        if (e.x != p.root_code) {
+          const float* box = (e.y == kNoHit) ? p.root_box
+                                             : reinterpret_cast<const float*>(p.nodes + size_t(e.y >> 1) * NL::vec) +
+                                                   (e.y & 1u) * 2 * D;
+          float blo[D], bhi[D], tb;
+#pragma unroll
+          for (int i = 0; i < D; ++i) {
+            blo[i] = box[i];
+            bhi[i] = box[D + i];
+          }
+          if (test_box(blo, bhi, tb)) {
+            // The root waits below the bucket; the bucket goes first.
+            s_code[tid] = p.root_code;
+            s_t[tid] = te;
+            L.sp = 1;
+            L.code = e.x;
+            L.skip = e.x;
+            if (STATS) L.v_nodes += 1;
+          }
+        }
+      }
+    }
+    return hit_root;
   };
 
   // Tests the primitives of the leaf in L.code.
@@ -455,11 +498,15 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
             else h = narrow_cast<D, N>(rec, L.r, L.pmin, L.pmax, L.limit, t, nrm);
             if (h) {
               if (STATS) L.v_hit += 1;
-              if (DETECT && N != kNarrowAabb) L.flag |= uint32_t(t < prim_entry<D, N, kCast>(rec, L.r, L.pmin, L.pmax, L.fast));
               if (L.best_leaf == kNoHit || hit_before(t, id, L.best_t, L.best_leaf)) {
                 L.best_leaf = id;
                 L.best_t = t;
-                L.limit = t;
+                if constexpr (DETECT) {
+                  L.limit = near_limit(t, p.window);
+                  L.best_pos = pos;
+                } else {
+                  L.limit = t;
+                }
 #pragma unroll
                 for (int i = 0; i < D; ++i) L.best_n[i] = nrm[i];
               }
@@ -508,11 +555,9 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
     }
   };
 
-  bool pending = false;  // this lane's query waits to be answered again in reference order
   for (;;) {
-    // Refill the lanes without a query: a pending replay restarts its own
-    // query in the reference order, the others take the next ones.
-    const bool need = !live && !exhausted && !pending;
+    // Refill the lanes without a query.
+    const bool need = !live && !exhausted;
     const uint32_t need_mask = __ballot_sync(FULL, need);
     uint32_t qs = kNoHit;
     if (need_mask) {
@@ -522,22 +567,15 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
       base = __shfl_sync(FULL, base, leader);
       if (need) {
         const uint32_t q = base + uint32_t(__popc(need_mask & lt_mask));
-        if (q < n_queries) qs = q;
+        if (q < n_queries) qs = p.q_list ? p.q_list[q] : q;
         else exhausted = true;
       }
     }
-    bool replay = false;
-    if (pending) {
-      qs = L.q;
-      pending = false;
-      replay = true;
-    }
     if (qs != kNoHit) {
-      L.ref = replay;
       live = start(qs);
       if (!live) finish();
     }
-    const uint32_t live_mask = __ballot_sync(FULL, live || pending);
+    const uint32_t live_mask = __ballot_sync(FULL, live);
     if (!live_mask) {
       if (__all_sync(FULL, exhausted)) break;
       continue;
@@ -551,13 +589,13 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
         const uint32_t ca = __float_as_uint(rec[4 * D]);
         const uint32_t cb = __float_as_uint(rec[4 * D + 1]);
         float ta, tb;
-        const bool pa = test_box(rec, rec + D, ta);
-        const bool pb = test_box(rec + 2 * D, rec + 3 * D, tb);
+        const bool pa = test_box(rec, rec + D, ta) && (!SEED || ca != L.skip);
+        const bool pb = test_box(rec + 2 * D, rec + 3 * D, tb) && (!SEED || cb != L.skip);
         if (STATS) L.v_nodes += 2;
         if (pa && pb) {
           // Reference order: child_a waits, child_b goes first. Near-first:
           // the smaller entry goes first.
-          const bool a_first = (REF || !kNearest) ? false : (!L.ref && ta <= tb);
+          const bool a_first = (REF || !kNearest) ? false : (ta <= tb);
           s_code[L.sp * kThreads + tid] = a_first ? cb : ca;
           s_t[L.sp * kThreads + tid] = a_first ? tb : ta;
           ++L.sp;
@@ -577,19 +615,9 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
       }
       if (done) {
         live = false;
-        if (DETECT && !L.ref && (L.flag != 0u || L.min_pruned <= near_limit(L.limit, p.window))) {
-          pending = true;  // answered again in reference order at the top of the loop
-          ++replays;
-        } else {
-          finish();
-        }
+        finish();
       }
     }
-  }
-  if (DETECT && p.replay_count) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) replays += __shfl_down_sync(FULL, replays, o);
-    if (lane == 0 && replays) atomicAdd(p.replay_count, replays);
   }
   if (STATS) {
 #pragma unroll
@@ -723,6 +751,7 @@ struct KernelSet {
   const void* cast_all;
   const void* overlap;
   const void* refit_leaves;
+  const void* ray_nearest_seeded[2];  // [stats]; D = 3 only
 };
 
 template <int D, int N> KernelSet make_kernel_set() {
@@ -738,6 +767,12 @@ template <int D, int N> KernelSet make_kernel_set() {
   s.cast_all = (const void*)query_kernel<D, N, kCastAll, true, false>;
   s.overlap = (const void*)query_kernel<D, N, kOverlap, true, false>;
   s.refit_leaves = (const void*)refit_kernel<D, N>;
+  s.ray_nearest_seeded[0] = nullptr;
+  s.ray_nearest_seeded[1] = nullptr;
+  if constexpr (D == 3) {
+    s.ray_nearest_seeded[0] = (const void*)query_kernel<D, N, kRayNearest, false, false, true>;
+    s.ray_nearest_seeded[1] = (const void*)query_kernel<D, N, kRayNearest, false, true, true>;
+  }
   return s;
 }
 

@@ -175,8 +175,17 @@ def terrain_scene(seed: int = 1, nx: int = 1024, ny: int = 512, n_coherent: int 
     tris = grid_triangles(verts)
     n_coh = nx * ny if n_coherent is None else n_coherent
     n_inc = nx * ny if n_incoherent is None else n_incoherent
-    # Coherent: one ray per camera-grid cell centre over the nx x ny grid
-    # (524,288 at full size; sub-sampled evenly when n_coh is smaller).
+    zmin, zmax = float(verts[..., 2].min()), float(verts[..., 2].max())
+    rays = terrain_rays(rng, nx, ny, zmin, zmax, n_coh, n_inc)
+    return dict(name="terrain", dim=3, kind="tris", prims=tris, rays=rays, max_toi=2000.0,
+                n_coherent=n_coh, waves=waves, all_hits_k=16, zrange=(zmin, zmax), grid=(nx, ny))
+
+
+def terrain_rays(rng: "Rng", nx: int, ny: int, zmin: float, zmax: float, n_coh: int, n_inc: int) -> np.ndarray:
+    """The terrain workload's two ray kinds: coherent rays from the nx x ny
+    camera grid at z = 200 jittered within 2 degrees of -z (cells sampled
+    evenly, repeating when n_coh exceeds the grid), then incoherent rays from
+    uniform origins in the scene box with isotropic directions."""
     cam = np.arange(n_coh, dtype=np.int64) * (nx * ny) // max(n_coh, 1)
     cx = (cam % nx).astype(np.float64) + 0.5
     cy = (cam // nx).astype(np.float64) + 0.5
@@ -185,16 +194,13 @@ def terrain_scene(seed: int = 1, nx: int = 1024, ny: int = 512, n_coherent: int 
     phi = 2.0 * math.pi * u[:, 1]
     d_coh = np.stack([np.sin(theta) * np.cos(phi), np.sin(theta) * np.sin(phi), -np.cos(theta)], axis=1)
     o_coh = np.stack([cx, cy, np.full(n_coh, 200.0)], axis=1)
-    zmin, zmax = float(verts[..., 2].min()), float(verts[..., 2].max())
     lo = np.array([0.0, 0.0, zmin])
     hi = np.array([float(nx), float(ny), zmax])
     o_inc = lo + (hi - lo) * rng.unit64((n_inc, 3))
     d_inc = rng.normal64((n_inc, 3))
     origins = np.concatenate([o_coh, o_inc]).astype(np.float32)
     dirs = np.concatenate([d_coh, d_inc]).astype(np.float32)
-    rays = rays_from(origins, dirs)
-    return dict(name="terrain", dim=3, kind="tris", prims=tris, rays=rays, max_toi=2000.0,
-                n_coherent=n_coh, waves=waves, all_hits_k=16)
+    return rays_from(origins, dirs)
 
 
 # ---------------------------------------------------------------------------

@@ -40,7 +40,7 @@ def test_boxes_nearest(boxes, order):
         ref = o.nearest(s["rays"], s["max_toi"], stats=order == sq.ORDER_REFERENCE)
         got = g.raycast_nearest(s["rays"], s["max_toi"], stats=order == sq.ORDER_REFERENCE)
     finally:
-        ctx().set_order(sq.ORDER_REFERENCE)
+        ctx().set_order(sq.ORDER_NEAR_FIRST)
     assert (ref.leaf != O.NO_HIT).mean() > 0.1
     assert_same_nearest(ref, got, label="boxes nearest")
     if order == sq.ORDER_REFERENCE:
@@ -80,7 +80,7 @@ def test_terrain_nearest_full(terrain, order):
     try:
         got = g.raycast_nearest(s["rays"], s["max_toi"])
     finally:
-        ctx().set_order(sq.ORDER_REFERENCE)
+        ctx().set_order(sq.ORDER_NEAR_FIRST)
     ref = o.nearest(s["rays"], s["max_toi"])
     assert (ref.leaf != O.NO_HIT).mean() > 0.5
     assert_same_nearest(ref, got, label="terrain nearest")

@@ -24,7 +24,7 @@ ORDERS = [sq.ORDER_NEAR_FIRST, sq.ORDER_REFERENCE]
 def order(request):
     ctx().set_order(request.param)
     yield request.param
-    ctx().set_order(sq.ORDER_REFERENCE)
+    ctx().set_order(sq.ORDER_NEAR_FIRST)
 
 
 @pytest.mark.parametrize("dim,seed,n,lo,hi", [(3, 0xABCD_1234, 64, -60.0, 60.0), (2, 0x2222_2222, 48, -60.0, 60.0),
@@ -98,7 +98,7 @@ def test_reference_order_replays_cpu_counters():
         want = ref.stats.sum(axis=0)
         assert [got.stats[k] for k in ("nodes_visited", "aabb_tests", "narrow_tests", "hits")] == list(want)
     finally:
-        ctx().set_order(sq.ORDER_REFERENCE)
+        ctx().set_order(sq.ORDER_NEAR_FIRST)
 
 
 def test_counters_known_answers():
@@ -108,7 +108,7 @@ def test_counters_known_answers():
     assert h.count[0] == 3 and list(h.stats.values()) == [1, 1, 3, 3]
     ctx().set_order(sq.ORDER_REFERENCE)
     n = g.raycast_nearest(axis_ray(), 100.0, stats=True)
-    ctx().set_order(sq.ORDER_REFERENCE)
+    ctx().set_order(sq.ORDER_NEAR_FIRST)
     assert n.leaf[0] == 0 and list(n.stats.values()) == [1, 1, 3, 1]
     m = g.raycast_all(np.array([0, 0, 0, 0, 0, 1], np.float32), 100.0, stats=True)
     assert m.count[0] == 0 and list(m.stats.values()) == [1, 1, 0, 0]

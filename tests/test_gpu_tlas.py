@@ -23,7 +23,7 @@ EYE3 = np.eye(3, dtype=np.float32)
 def order(request):
     ctx().set_order(request.param)
     yield request.param
-    ctx().set_order(sq.ORDER_REFERENCE)
+    ctx().set_order(sq.ORDER_NEAR_FIRST)
 
 
 def tpair(kind, dim, rot, trans, param, layers=None, sub=None):
@@ -157,7 +157,7 @@ def test_reference_order_counters_match():
         assert_same_nearest(ref, got, sub=False)
         assert list(got.stats.values()) == list(ref.stats.sum(axis=0))
     finally:
-        ctx().set_order(sq.ORDER_REFERENCE)
+        ctx().set_order(sq.ORDER_NEAR_FIRST)
 
 
 # -- instanced meshes (the two-level benchmark scene) -------------------------
