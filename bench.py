@@ -7,13 +7,20 @@ against a 1,048,576-triangle height field (1024 x 512 cells, 6 random-phase
 sinusoids of amplitude 1-20 plus N(0, 0.5) noise), t_max 2000; seeded
 synthetic data (the reference publishes no dataset).
 
-Metric: Mrays/s. ``value`` is device-timed throughput with rays resident in
-HBM (CUDA events around each launch on the launching stream, L2 flushed by a
-256 MiB write between steps, outside the timed events); ``e2e`` is the same
-metric through the host-buffer C ABI call (pinned host rays in, leaf / toi /
-normal out, copies inside the timed region). Multi-GPU runs are weak-scaled:
-every rank answers its own 1,048,576-ray batch against its own replica of
-the scene, with no collective on the data path; time is the max over ranks.
+Metric: Mrays/s of the learned-seeded query (the guide network's fused
+tcgen05 inference, then the traversal seeded by its predicted bucket), with
+the plain GPU traversal of the same rays timed beside it and the hits of the
+two checked bit-identical. The guide (4,096 buckets = depth-12 subtrees) is
+trained before timing on 4,194,304 rays of the same two kinds (another seed)
+labelled by the plain traversal: AdamW, lr 1e-3, batch 8192.
+
+``value`` is device-timed throughput with rays resident in HBM (CUDA events
+around each step on the launching stream, L2 flushed by a 256 MiB write
+between steps, outside the timed events); ``e2e`` is the same metric through
+the host-buffer C ABI call (pinned host rays in, leaf / toi / normal out,
+copies inside the timed region). Multi-GPU runs are weak-scaled: every rank
+answers its own 1,048,576-ray batch against its own replica of the scene,
+with no collective on the data path; time is the max over ranks.
 
 ``--impl reference`` times the reference's CPU algorithm (the oracle's C++
 restatement of Bvh::raycast_nearest_batch_parallel, all host threads) on a
@@ -38,6 +45,7 @@ METRIC = "Mrays/s nearest-hit, 1M tris; learned-seeded vs plain GPU, identical h
 WORKLOAD = ("terrain height field 1024x512 cells = 1,048,576 triangles; 1,048,576 rays per step "
             "(524,288 coherent + 524,288 incoherent); raycast_nearest, t_max 2000, default filter")
 RAY_BYTES = 24    # origin[3], dir[3] f32
+MLP_MACS = 6 * 128 + 2 * 128 * 128 + 128 * 4096  # multiply-adds per ray of the guide network
 OUT_BYTES = 20    # leaf u32, toi f32, normal[3] f32
 
 
@@ -48,6 +56,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--order", default="near_first", choices=["near_first", "reference"])
+    ap.add_argument("--train-rays", type=int, default=1 << 22, help="guide training rays (labelled by plain traversal)")
+    ap.add_argument("--epochs", type=int, default=2, help="guide training epochs (batch 8192, AdamW lr 1e-3)")
     ap.add_argument("--rays", type=int, default=1 << 20,
                     help="rays per step (half coherent, half incoherent); the metric is quoted at 1,048,576")
     return ap.parse_args()
@@ -118,6 +128,15 @@ def measured_peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def tensor_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["bf16_tflops"]), "measured (cuBLAS bf16 burst)"
+    return 1590.0, "fallback"
 
 
 def profiled_traffic():
@@ -191,6 +210,19 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def timed(stream, fn, steps, flush):
+    """Mean device time (ms) of fn over `steps` launches, L2 flushed before each."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for i in range(steps):
+        flush.fill_(i & 0xFF)
+        ev[i][0].record(stream)
+        fn()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -198,6 +230,7 @@ def main():
         run_reference(args, rank, world)
         return
 
+    import ctypes as C
     import torch
     import spatial_query_b200 as sq
     from spatial_query_b200 import scenes
@@ -212,8 +245,8 @@ def main():
     s = scenes.terrain_scene(seed=1)
     if rank > 0:
         # Weak scaling: each rank its own ray batch of the same two kinds.
-        s2 = scenes.terrain_scene(seed=1 + 1000 * rank)
-        s["rays"] = s2["rays"]
+        nx, ny = s["grid"]
+        s["rays"] = scenes.terrain_rays(scenes.Rng(1 + 1000 * rank), nx, ny, *s["zrange"], nx * ny, nx * ny)
     if args.rays != s["rays"].shape[0]:
         half, total = args.rays // 2, s["rays"].shape[0]
         s["rays"] = np.ascontiguousarray(np.concatenate([s["rays"][:half], s["rays"][total // 2: total // 2 + half]]))
@@ -227,113 +260,198 @@ def main():
     ctx.set_order(sq.ORDER_REFERENCE if args.order == "reference" else sq.ORDER_NEAR_FIRST)
     scene = sq.DeviceBvh(ctx, tree, geom)
     info = scene.info()
-
     dev = torch.device("cuda", local)
     d_rays = torch.from_numpy(s["rays"]).to(dev)
     d_leaf = torch.empty(n, dtype=torch.int32, device=dev)
     d_toi = torch.empty(n, dtype=torch.float32, device=dev)
     d_nrm = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    g_leaf, g_toi, g_nrm = torch.empty_like(d_leaf), torch.empty_like(d_toi), torch.empty_like(d_nrm)
+    d_bucket = torch.empty(n, dtype=torch.int32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
-    def step():
+    # The learned guide, trained before timing on its own rays (same two
+    # kinds, another seed), labelled by the plain traversal.
+    t0 = time.perf_counter()
+    nx, ny = s["grid"]
+    n_train = args.train_rays
+    train = scenes.terrain_rays(scenes.Rng(4 + 1000 * rank), nx, ny, *s["zrange"], n_train // 2, n_train // 2)
+    d_train = torch.from_numpy(train).to(dev)
+    d_lab = torch.empty(n_train, dtype=torch.int32, device=dev)
+    guide = sq.Guide(scene, seed=rank)
+    guide.label_d(d_train, n_train, s["max_toi"], d_lab)
+    losses = guide.train_d(d_train, d_lab, n_train, args.epochs)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    del d_train, d_lab
+
+    def plain():
         scene.raycast_nearest_d(d_rays, n, s["max_toi"], d_leaf, d_toi, d_nrm)
 
-    # Instrumented run (untimed): per-batch counters for the algorithmic bytes.
+    def guided():
+        guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], g_leaf, g_toi, g_nrm)
+
+    def predict():
+        guide.predict_d(d_rays, n, d_bucket)
+
+    def seeded():
+        guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], g_leaf, g_toi, g_nrm, d_bucket=d_bucket)
+
+    # Instrumented runs (untimed): counters for the algorithmic bytes, and
+    # the identical-hits check.
     st = scene.raycast_nearest_d(d_rays, n, s["max_toi"], d_leaf, d_toi, d_nrm, stats=True)
-    torch.cuda.synchronize()
     replayed = ctx.last_replay_count if args.order == "near_first" else 0
-    fetches = (st["nodes_visited"] - n) // 2          # child-pair records read
-    alg_bytes = (fetches * info["node_record_bytes"] + st["narrow_tests"] * info["prim_record_bytes"]
-                 + n * (RAY_BYTES + OUT_BYTES))
+    predict()
+    st_g = guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], g_leaf, g_toi, g_nrm, d_bucket=d_bucket,
+                                          stats=True)
+    replayed_g = ctx.last_replay_count
+    torch.cuda.synchronize()
+    identical = bool(torch.equal(g_leaf, d_leaf) and torch.equal(g_toi.view(torch.int32), d_toi.view(torch.int32))
+                     and torch.equal(g_nrm.view(torch.int32), d_nrm.view(torch.int32)))
+    if not identical:
+        raise SystemExit("learned-seeded hits differ from the plain query's")
+    d_lt = torch.empty(n, dtype=torch.int32, device=dev)
+    guide.label_d(d_rays, n, s["max_toi"], d_lt)
+    torch.cuda.synchronize()
+    hit = d_lt >= 0
+    top1 = float((d_bucket[hit] == d_lt[hit]).float().mean().item())
+    del d_lt
+
+    def record_bytes(stats):
+        fetches = (stats["nodes_visited"] - n) // 2  # child-pair records read
+        return fetches, (fetches * info["node_record_bytes"] + stats["narrow_tests"] * info["prim_record_bytes"]
+                         + n * (RAY_BYTES + OUT_BYTES))
+
+    fetches, alg_bytes = record_bytes(st)
+    fetches_g, alg_bytes_g = record_bytes(st_g)
 
     for _ in range(args.warmup):
         flush.fill_(1)
-        step()
+        plain()
+        flush.fill_(2)
+        guided()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     launches0 = ctx.launch_count
     with ClockSampler(local) as clk:
-        for i in range(args.steps):
-            flush.fill_(i & 0xFF)
-            ev[i][0].record(stream)
-            step()
-            ev[i][1].record(stream)
-        torch.cuda.synchronize()
+        g_ms = timed(stream, guided, args.steps, flush)
     launches = ctx.launch_count - launches0
+    p_ms = timed(stream, plain, args.steps, flush)
+    pr_ms = timed(stream, predict, args.steps, flush)
+    sd_ms = timed(stream, seeded, args.steps, flush)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    ms = sum(step_ms) / len(step_ms)
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+
+    def mean_max(xs):
+        m = sum(xs) / len(xs)
+        if dist:
+            t = torch.tensor([m], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            m = float(t.item())
+        return m
+
+    ms, plain_ms, predict_ms, seeded_ms = mean_max(g_ms), mean_max(p_ms), mean_max(pr_ms), mean_max(sd_ms)
     value = world * n / (ms / 1000) / 1e6
+    plain_value = world * n / (plain_ms / 1000) / 1e6
 
     # End to end through the host-buffer C ABI: pinned rays in, hits out.
     h_rays = torch.from_numpy(s["rays"]).pin_memory()
     h_leaf = torch.empty(n, dtype=torch.int32).pin_memory()
     h_toi = torch.empty(n, dtype=torch.float32).pin_memory()
     h_nrm = torch.empty((n, 3), dtype=torch.float32).pin_memory()
-    import ctypes as C
     hits = sq._Hits(h_leaf.data_ptr(), h_toi.data_ptr(), None, h_nrm.data_ptr(), None)
 
-    def e2e_step():
+    def e2e_guided():
+        ctx.check(sq.lib().sq_raycast_nearest_guided(ctx.h, scene.h, guide.h, h_rays.data_ptr(), n, s["max_toi"],
+                                                      C.byref(hits), None), "sq_raycast_nearest_guided")
+
+    def e2e_plain():
         ctx.check(sq.lib().sq_raycast_nearest(ctx.h, scene.h, h_rays.data_ptr(), n, s["max_toi"], None, None,
                                               C.byref(hits), None), "sq_raycast_nearest")
 
-    for _ in range(max(2, args.warmup)):
-        e2e_step()
-    torch.cuda.synchronize()
-    e_ms = []
-    for i in range(args.steps):
-        flush.fill_(i & 0xFF)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        e2e_step()
-        b.record(stream)
-        b.synchronize()
-        e_ms.append(a.elapsed_time(b))
-    e2e_ms = sum(e_ms) / len(e_ms)
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * n / (e2e_ms / 1000) / 1e6
-    # The e2e results equal the device-resident results.
+    def e2e_time(fn):
+        for _ in range(max(2, args.warmup)):
+            fn()
+        out = []
+        for i in range(args.steps):
+            flush.fill_(i & 0xFF)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            out.append(a.elapsed_time(b))
+        return mean_max(out)
+
+    e2e_ms = e2e_time(e2e_guided)
     assert torch.equal(h_leaf, d_leaf.cpu()) and torch.equal(h_toi.view(torch.int32), d_toi.cpu().view(torch.int32))
+    e2e_plain_ms = e2e_time(e2e_plain)
+    e2e_value = world * n / (e2e_ms / 1000) / 1e6
 
     peak, peak_kind = measured_peaks()
-    achieved = alg_bytes / (ms / 1000) / 1e9
+    tpeak = tensor_peak()
+    mlp_flop = 2 * MLP_MACS * n
+    infer_tflops = mlp_flop / (predict_ms / 1000) / 1e12
+    achieved = alg_bytes / (plain_ms / 1000) / 1e9
+    achieved_g = alg_bytes_g / (seeded_ms / 1000) / 1e9
     traffic = profiled_traffic()
     cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_baseline_sample(s, os.cpu_count() or 1)
 
     if rank == 0:
+        roof_trav = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                     "kernel": "query_kernel<3, tri, nearest> (plain, near-first)",
+                     "alg_bytes_per_launch": int(alg_bytes), "alg_bytes_per_ray": round(alg_bytes / n, 1),
+                     "counts_per_ray": {"node_records": round(fetches / n, 2),
+                                        "narrow_tests": round(st["narrow_tests"] / n, 2)}}
+        roof_mlp = {"bound": "tensor", "achieved": round(infer_tflops, 1), "peak": tpeak[0], "unit": "TFLOP/s",
+                    "frac": round(infer_tflops / tpeak[0], 4), "traffic": None, "peak_source": tpeak[1],
+                    "kernel": "guide_infer_kernel (fused MLP + argmax)",
+                    "flop_per_ray": 2 * MLP_MACS, "ms": round(predict_ms, 4)}
+        roof_seed = {"bound": "hbm", "achieved": round(achieved_g, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved_g / peak, 4), "peak_source": peak_kind,
+                     "kernel": "query_kernel<3, tri, nearest, SEED>", "ms": round(seeded_ms, 4),
+                     "alg_bytes_per_ray": round(alg_bytes_g / n, 1),
+                     "counts_per_ray": {"node_records": round(fetches_g / n, 2),
+                                        "narrow_tests": round(st_g["narrow_tests"] / n, 2)}}
+        dominant = roof_mlp if predict_ms >= seeded_ms else roof_seed
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded height field and rays)",
-            "config": {"workload": WORKLOAD, "path": f"plain GPU traversal, {args.order} order",
-                       "replayed_in_reference_order": int(replayed),
+            "vs_baseline": None, "dtype": "f32 (traversal), bf16 x bf16 -> f32 (guide MLP)",
+            "data": "synthetic (seeded height field and rays)",
+            "config": {"workload": WORKLOAD,
+                       "path": f"learned-seeded: fused tcgen05 MLP inference + seeded {args.order} traversal",
+                       "identical_hits": identical,
+                       "plain_gpu": {"value": round(plain_value, 3), "unit": "Mrays/s", "ms_per_step": round(plain_ms, 4),
+                                     "path": f"plain GPU traversal, {args.order} order",
+                                     "e2e_mrays": round(world * n / (e2e_plain_ms / 1000) / 1e6, 3),
+                                     "replayed_in_reference_order": int(replayed)},
+                       "learned_vs_plain": round(value / plain_value, 4),
+                       "breakdown_ms": {"inference": round(predict_ms, 4), "seeded_traversal": round(seeded_ms, 4),
+                                        "plain_traversal": round(plain_ms, 4)},
+                       "nodes_visited_per_ray": {"plain": round(st["nodes_visited"] / n, 3),
+                                                 "learned_seeded": round(st_g["nodes_visited"] / n, 3)},
+                       "guide": {"buckets": guide.info()["n_buckets"], "train_rays": n_train,
+                                 "epochs": args.epochs, "batch": guide.batch, "optimizer": "AdamW lr 1e-3",
+                                 "loss_per_epoch": [round(float(x), 4) for x in losses],
+                                 "train_seconds": round(train_s, 2), "top1_on_hits": round(top1, 4),
+                                 "replayed_in_reference_order": int(replayed_g)},
                        "l2": "flushed between steps (256 MiB write, outside the timed events)",
                        "parallelism": f"replicated scene, rays sharded per rank (dp{world})",
                        "tree": {"nodes": info["n_nodes"], "depth": info["max_depth"],
                                 "node_record_bytes": info["node_record_bytes"],
                                 "prim_record_bytes": info["prim_record_bytes"]}},
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
-                         "alg_bytes_per_launch": int(alg_bytes),
-                         "alg_bytes_per_ray": round(alg_bytes / n, 1),
-                         "counts_per_ray": {"node_records": round(fetches / n, 2),
-                                            "narrow_tests": round(st["narrow_tests"] / n, 2)}},
+            "roofline": dominant,
+            "roofline_kernels": {"mlp_inference": roof_mlp, "seeded_traversal": roof_seed,
+                                 "plain_traversal": roof_trav},
             "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": n * RAY_BYTES,
-                    "d2h_bytes_per_step": n * OUT_BYTES, "ms_per_step": round(e2e_ms, 4)},
+                    "d2h_bytes_per_step": n * OUT_BYTES, "ms_per_step": round(e2e_ms, 4),
+                    "call": "sq_raycast_nearest_guided (host buffers)"},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
         }
@@ -343,6 +461,7 @@ def main():
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+    guide.close()
     scene.close()
     ctx.close()
 

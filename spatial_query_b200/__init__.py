@@ -141,6 +141,25 @@ SIGNATURES = {
     "sq_graph_end": (C.c_int32, [P, C.POINTER(P)]),
     "sq_graph_launch": (C.c_int32, [P, P]),
     "sq_graph_destroy": (C.c_int32, [P]),
+    # learned guide (include/sq_guide.h)
+    "sq_guide_config_default": (None, [P]),
+    "sq_guide_create": (C.c_int32, [P, P, P, C.POINTER(P)]),
+    "sq_guide_destroy": (C.c_int32, [P]),
+    "sq_guide_get_info": (C.c_int32, [P, P]),
+    "sq_guide_label_d": (C.c_int32, [P, P, C.c_uint32, C.c_float, P]),
+    "sq_guide_train_step_d": (C.c_int32, [P, P, P, C.POINTER(C.c_float)]),
+    "sq_guide_train_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_uint32, P]),
+    "sq_guide_forward_backward_d": (C.c_int32, [P, P, P, C.POINTER(C.c_float)]),
+    "sq_guide_get_params": (C.c_int32, [P, P, C.c_uint64]),
+    "sq_guide_set_params": (C.c_int32, [P, P, C.c_uint64]),
+    "sq_guide_get_grads": (C.c_int32, [P, P, C.c_uint64]),
+    "sq_guide_predict_d": (C.c_int32, [P, P, C.c_uint32, P]),
+    "sq_raycast_nearest_guided_d": (C.c_int32, [P, P, P, P, C.c_uint32, C.c_float, P, P, P]),
+    "sq_raycast_nearest_guided": (C.c_int32, [P, P, P, P, C.c_uint32, C.c_float, P, P]),
+    "sq_guide_save": (C.c_int32, [P, P, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "sq_guide_load": (C.c_int32, [P, P, C.c_size_t]),
+    "sq_gemm_bf16_tn_d": (C.c_int32, [P, P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                      C.c_uint32]),
 }
 
 INSTANCE = {"mesh": 0, "box": 1, "ball": 2}
@@ -790,3 +809,119 @@ class DeviceTlas:
                    _p(regions), n_regions, region_k, _p(region_count), _p(region_leaves))
         self.ctx.check(lib().sq_tlas_mixed_d(self.ctx.h, self.h, C.byref(m), _filter(mask, exclude)),
                        "sq_tlas_mixed_d")
+
+
+# ---------------------------------------------------------------------------
+# Learned guide (include/sq_guide.h)
+# ---------------------------------------------------------------------------
+
+class _GuideConfig(C.Structure):
+    _fields_ = [("depth", C.c_uint32), ("batch", C.c_uint32), ("lr", C.c_float), ("weight_decay", C.c_float),
+                ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float), ("seed", C.c_uint64)]
+
+
+class _GuideInfo(C.Structure):
+    _fields_ = [("n_buckets", C.c_uint32), ("n_out", C.c_uint32), ("hidden", C.c_uint32), ("inputs", C.c_uint32),
+                ("n_params", C.c_uint64), ("steps", C.c_uint32)]
+
+
+class Guide:
+    """The learned guide of a D = 3 scene: an MLP that predicts, per ray, the
+    bucket (subtree at ``depth``) holding its nearest hit, trained and run on
+    the GPU; ``raycast_nearest_guided_d`` returns the same hits as the plain
+    query. Device arrays are torch tensors on the scene's device."""
+
+    def __init__(self, scene: "DeviceBvh", depth: int = 12, batch: int = 8192, lr: float = 1e-3,
+                 weight_decay: float = 0.01, seed: int = 0):
+        cfg = _GuideConfig()
+        lib().sq_guide_config_default(C.byref(cfg))
+        cfg.depth, cfg.batch, cfg.lr, cfg.weight_decay, cfg.seed = depth, batch, lr, weight_decay, seed
+        h = P()
+        scene.ctx.check(lib().sq_guide_create(scene.ctx.h, scene.h, C.byref(cfg), C.byref(h)), "guide_create")
+        self.h, self.scene, self.ctx, self.batch = h, scene, scene.ctx, batch
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.sq_guide_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def info(self) -> dict:
+        i = _GuideInfo()
+        self.ctx.check(lib().sq_guide_get_info(self.h, C.byref(i)), "guide_info")
+        return {k: getattr(i, k) for k, _ in _GuideInfo._fields_}
+
+    def label_d(self, d_rays, n, max_toi, d_labels):
+        self.ctx.check(lib().sq_guide_label_d(self.h, _p(d_rays), n, float(max_toi), _p(d_labels)), "guide_label")
+
+    def train_step_d(self, d_rays, d_labels) -> float:
+        loss = C.c_float(0.0)
+        self.ctx.check(lib().sq_guide_train_step_d(self.h, _p(d_rays), _p(d_labels), C.byref(loss)), "train_step")
+        return float(loss.value)
+
+    def train_d(self, d_rays, d_labels, n, epochs) -> np.ndarray:
+        losses = np.zeros(max(epochs, 1), np.float32)
+        self.ctx.check(lib().sq_guide_train_d(self.h, _p(d_rays), _p(d_labels), n, epochs, _p(losses)), "train")
+        return losses[:epochs]
+
+    def forward_backward_d(self, d_rays, d_labels) -> float:
+        loss = C.c_float(0.0)
+        self.ctx.check(lib().sq_guide_forward_backward_d(self.h, _p(d_rays), _p(d_labels), C.byref(loss)),
+                       "forward_backward")
+        return float(loss.value)
+
+    def _vec(self, fn) -> np.ndarray:
+        out = np.empty(self.info()["n_params"], np.float32)
+        self.ctx.check(getattr(lib(), fn)(self.h, _p(out), out.size), fn)
+        return out
+
+    def get_params(self) -> np.ndarray:
+        return self._vec("sq_guide_get_params")
+
+    def get_grads(self) -> np.ndarray:
+        return self._vec("sq_guide_get_grads")
+
+    def set_params(self, v):
+        v = _f32(v)
+        self.ctx.check(lib().sq_guide_set_params(self.h, _p(v), v.size), "set_params")
+
+    def predict_d(self, d_rays, n, d_bucket):
+        self.ctx.check(lib().sq_guide_predict_d(self.h, _p(d_rays), n, _p(d_bucket)), "predict")
+
+    def raycast_nearest_guided_d(self, d_rays, n, max_toi, d_leaf, d_toi=None, d_normal=None, d_bucket=None,
+                                 stats=False):
+        s = _Hits(_p(d_leaf), _p(d_toi), None, _p(d_normal), None)
+        st = _Stats() if stats else None
+        self.ctx.check(lib().sq_raycast_nearest_guided_d(self.ctx.h, self.scene.h, self.h, _p(d_rays), n,
+                                                          float(max_toi), _p(d_bucket), C.byref(s),
+                                                          C.byref(st) if st else None), "raycast_nearest_guided_d")
+        return _stats_dict(st) if st else None
+
+    def raycast_nearest_guided(self, rays, max_toi) -> "Hits":
+        rays = _f32(rays).reshape(-1, 6)
+        n = rays.shape[0]
+        h = Hits(np.empty(n, np.uint32), np.empty(n, np.float32))
+        h.normal = np.empty((n, 3), np.float32)
+        h.point = np.empty((n, 3), np.float32)
+        s = _Hits(_p(h.leaf), _p(h.toi), None, _p(h.normal), _p(h.point))
+        self.ctx.check(lib().sq_raycast_nearest_guided(self.ctx.h, self.scene.h, self.h, _p(rays), n,
+                                                        float(max_toi), C.byref(s), None), "raycast_nearest_guided")
+        return h
+
+    def save(self) -> bytes:
+        size = C.c_size_t(0)
+        self.ctx.check(lib().sq_guide_save(self.h, None, 0, C.byref(size)), "save")
+        buf = (C.c_uint8 * size.value)()
+        self.ctx.check(lib().sq_guide_save(self.h, buf, size.value, C.byref(size)), "save")
+        return bytes(buf)
+
+    def load(self, blob: bytes):
+        buf = (C.c_uint8 * len(blob)).from_buffer_copy(blob)
+        self.ctx.check(lib().sq_guide_load(self.h, buf, len(blob)), "load")
+
+
+def gemm_bf16_tn_d(ctx: Context, a, b, c, m, n, k, lda, ldb, ldc):
+    """C[m x n] (f32) = A[m x k] * B[n x k]^T on the tcgen05 GEMM (bf16 torch tensors)."""
+    ctx.check(lib().sq_gemm_bf16_tn_d(ctx.h, _p(a), _p(b), _p(c), m, n, k, lda, ldb, ldc), "gemm_bf16_tn_d")

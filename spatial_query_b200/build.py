@@ -29,6 +29,7 @@ UNITS = [
     ("kernels_d6.cu", ["--fmad=false"]),
     ("sq_tlas.cu", ["--fmad=false"]),
     ("tlas_kernels.cu", ["--fmad=false"]),
+    ("guide.cu", []),
     ("tree_build.cpp", []),
 ]
 
