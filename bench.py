@@ -143,10 +143,10 @@ def tensor_peak():
     return 1590.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per launch of the traversal kernel from the committed ncu
-    summary (profiles/ray_nearest_terrain.md), or None."""
-    p = os.path.join(ROOT, "profiles", "ray_nearest_terrain.md")
+def profiled_traffic(name: str):
+    """DRAM bytes per launch of a kernel from its committed ncu summary
+    (the `traffic_bytes_per_launch` line of profiles/<name>), or None."""
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -174,6 +174,23 @@ def cpu_baseline_sample(s, threads: int):
     return dict(value=n / dt / 1e6, unit="Mrays/s", cores=threads, kind="port",
                 sample=f"all {n} rays of the workload, one pass, {threads} threads, contiguous chunks "
                        f"(Bvh::raycast_nearest_batch_parallel semantics); tree build {build_s:.2f} s not counted")
+
+
+def f64_delta(s, leaf, toi, threads: int):
+    """The GPU's f32 answers against an f64 build of the reference's
+    algorithm (the oracle at double precision) on the same f32 inputs."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    sc = O.Scene("tris", 3, s["prims"], prec=64)
+    ref = sc.nearest(s["rays"], s["max_toi"], threads=threads)
+    same = (ref.leaf == leaf) & (leaf != O.NO_HIT)
+    dt = np.abs(toi[same].astype(np.float64) - ref.toi[same])
+    rel = dt / np.maximum(np.abs(ref.toi[same]), 1e-30)
+    return {"rays": int(len(leaf)), "same_leaf": round(float((ref.leaf == leaf).mean()), 6),
+            "max_abs_dt": float(dt.max()) if dt.size else 0.0, "max_rel_dt": float(rel.max()) if rel.size else 0.0,
+            "mean_rel_dt": float(rel.mean()) if rel.size else 0.0,
+            "note": "f32 GPU answers (bit-equal to the f32 reference) vs the f64 oracle; leaves differ only "
+                    "where two hits lie within f32 rounding of each other"}
 
 
 def run_reference(args, rank, world):
@@ -522,10 +539,13 @@ def main():
     infer_tflops = mlp_flop / (predict_ms / 1000) / 1e12
     achieved = alg_bytes / (plain_ms / 1000) / 1e9
     achieved_g = alg_bytes_g / (seeded_ms / 1000) / 1e9
-    traffic = profiled_traffic()
+    traffic = profiled_traffic("ray_nearest_terrain.md")
+    traffic_mlp = profiled_traffic("learned_seeded_terrain.md")
     cpu = None
+    f64 = None
     if rank == 0 and world == 1:
         cpu = cpu_baseline_sample(s, os.cpu_count() or 1)
+        f64 = f64_delta(s, d_leaf.cpu().numpy().view(np.uint32), d_toi.cpu().numpy(), os.cpu_count() or 1)
 
     if rank == 0:
         roof_trav = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -535,7 +555,7 @@ def main():
                      "counts_per_ray": {"node_records": round(fetches / n, 2),
                                         "narrow_tests": round(st["narrow_tests"] / n, 2)}}
         roof_mlp = {"bound": "tensor", "achieved": round(infer_tflops, 1), "peak": tpeak[0], "unit": "TFLOP/s",
-                    "frac": round(infer_tflops / tpeak[0], 4), "traffic": None, "peak_source": tpeak[1],
+                    "frac": round(infer_tflops / tpeak[0], 4), "traffic": traffic_mlp, "peak_source": tpeak[1],
                     "kernel": "guide_infer_kernel (fused MLP + argmax)",
                     "flop_per_ray": 2 * MLP_MACS, "ms": round(predict_ms, 4)}
         roof_seed = {"bound": "hbm", "achieved": round(achieved_g, 1), "peak": peak, "unit": "GB/s",
@@ -583,6 +603,8 @@ def main():
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if f64:
+            line["config"]["f64_reference"] = f64
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

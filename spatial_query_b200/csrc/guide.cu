@@ -454,14 +454,15 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
         if (j < 3) {
           // bias + ReLU -> bf16 -> next layer's operand rows
           const float* b = s_bias + j * 128;
-#pragma unroll 1
+          float v[128];
+          umma::tmem_ld128(tcol, v);  // the whole row in one load and one wait
+#pragma unroll
           for (uint32_t c = 0; c < 128; c += 32) {
-            float v[32];
-            umma::tmem_ld32(tcol + c, v);
             __align__(16) __nv_bfloat162 o[16];
 #pragma unroll
             for (int i = 0; i < 16; ++i)
-              o[i] = __floats2bfloat162_rn(fmaxf(v[2 * i] + b[c + 2 * i], 0.f), fmaxf(v[2 * i + 1] + b[c + 2 * i + 1], 0.f));
+              o[i] = __floats2bfloat162_rn(fmaxf(v[c + 2 * i] + b[c + 2 * i], 0.f),
+                                           fmaxf(v[c + 2 * i + 1] + b[c + 2 * i + 1], 0.f));
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
               const uint32_t k = c + 8 * i;
@@ -477,24 +478,25 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
           const uint32_t c0 = (j - 3) * 128;
           float m = -INFINITY;
           const bool full = c0 + 128 <= p.n_buckets;
-#pragma unroll 1
-          for (uint32_t c = 0; c < 128; c += 32) {
-            float v[32];
-            umma::tmem_ld32(tcol + c, v);
-            if (full) {
+          float v[128];
+          umma::tmem_ld128(tcol, v);  // the chunk's 128 logits of this row in one load and one wait
+          if (full) {
+            float m1 = -INFINITY;  // two independent max chains
 #pragma unroll
-              for (int i = 0; i < 32; i += 2) {
-                const float k0 = __uint_as_float((__float_as_uint(v[i]) & 0xFFFFFF80u) | (127u - (c + i)));
-                const float k1 = __uint_as_float((__float_as_uint(v[i + 1]) & 0xFFFFFF80u) | (126u - (c + i)));
-                m = umma::fmax3(m, k0, k1);
-              }
-            } else {
+            for (uint32_t i = 0; i < 128; i += 4) {
+              const float k0 = __uint_as_float((__float_as_uint(v[i]) & 0xFFFFFF80u) | (127u - i));
+              const float k1 = __uint_as_float((__float_as_uint(v[i + 1]) & 0xFFFFFF80u) | (126u - i));
+              const float k2 = __uint_as_float((__float_as_uint(v[i + 2]) & 0xFFFFFF80u) | (125u - i));
+              const float k3 = __uint_as_float((__float_as_uint(v[i + 3]) & 0xFFFFFF80u) | (124u - i));
+              m = umma::fmax3(m, k0, k1);
+              m1 = umma::fmax3(m1, k2, k3);
+            }
+            m = fmaxf(m, m1);
+          } else {
 #pragma unroll
-              for (int i = 0; i < 32; ++i) {
-                const uint32_t idx = c + i;
-                const float l = (c0 + idx < p.n_buckets) ? v[i] : -INFINITY;
-                m = fmaxf(m, __uint_as_float((__float_as_uint(l) & 0xFFFFFF80u) | (127u - idx)));
-              }
+            for (uint32_t i = 0; i < 128; ++i) {
+              const float l = (c0 + i < p.n_buckets) ? v[i] : -INFINITY;
+              m = fmaxf(m, __uint_as_float((__float_as_uint(l) & 0xFFFFFF80u) | (127u - i)));
             }
           }
           if (m > best) {
@@ -506,19 +508,16 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
         const uint32_t jn = j + 2;
         if (jn >= 3 && jn < 3 + p.n_chunks) {
           const float* b = s_bias + 384 + (jn - 3) * 128;
-#pragma unroll 1
-          for (uint32_t c = 0; c < 128; c += 32) {
-            float v[32];
+          float v[128];
 #pragma unroll
-            for (int i = 0; i < 32; i += 4) {
-              const float4 q4 = *reinterpret_cast<const float4*>(b + c + i);
-              v[i] = q4.x;
-              v[i + 1] = q4.y;
-              v[i + 2] = q4.z;
-              v[i + 3] = q4.w;
-            }
-            umma::tmem_st32(tcol + c, v);
+          for (int i = 0; i < 128; i += 4) {
+            const float4 q4 = *reinterpret_cast<const float4*>(b + i);
+            v[i] = q4.x;
+            v[i + 1] = q4.y;
+            v[i + 2] = q4.z;
+            v[i + 3] = q4.w;
           }
+          umma::tmem_st128(tcol, v);  // one store and one wait
         }
         umma::tc_fence_before();
         if (j < 3) umma::fence_proxy_async();
