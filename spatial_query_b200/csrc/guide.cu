@@ -308,12 +308,15 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
   uint64_t* w_full = bars + 0;
   uint64_t* ring_full = bars + 1;            // [3]
   uint64_t* ring_empty = bars + 4;           // [3]
-  uint64_t* acc_full = bars + 7;             // [2]
-  uint64_t* acc_empty = bars + 9;            // [2]
-  uint64_t* act_ready = bars + 11;
-  uint64_t* fin = bars + 12;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 13);
-  int* s_err = reinterpret_cast<int*>(bars + 14);
+  // The two 128-ray halves of a tile run as independent pipelines that
+  // share the weight ring: per stage and half an accumulator-full and an
+  // accumulator-empty barrier, per half an operand-ready barrier.
+  uint64_t* acc_full = bars + 7;             // [stage * 2 + half]
+  uint64_t* acc_empty = bars + 11;           // [stage * 2 + half]
+  uint64_t* act_ready = bars + 15;           // [half]
+  uint64_t* fin = bars + 17;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 18);
+  int* s_err = reinterpret_cast<int*>(bars + 19);
   const float* s_bias = reinterpret_cast<const float*>(base + InferSmem::bias);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -327,11 +330,12 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
       umma::mbar_init(&ring_full[s], 1);
       umma::mbar_init(&ring_empty[s], 1);
     }
-    for (int s = 0; s < 2; ++s) {
-      umma::mbar_init(&acc_full[s], 1);
-      umma::mbar_init(&acc_empty[s], 8);
+    for (int k = 0; k < 4; ++k) {
+      umma::mbar_init(&acc_full[k], 1);
+      umma::mbar_init(&acc_empty[k], 4);
     }
-    umma::mbar_init(act_ready, 8);
+    umma::mbar_init(&act_ready[0], 4);
+    umma::mbar_init(&act_ready[1], 4);
     umma::mbar_init(fin, 1);
     *s_err = 0;
     umma::fence_barrier_init();
@@ -373,24 +377,29 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
     if (lane == 0) {
       // MMA issuer.
       if (!umma::mbar_wait(w_full, 0)) set_err(2);
-      uint32_t G = 0, J = 0, A = 0;
+      uint32_t G = 0, J = 0, A[2] = {0u, 0u};
       const uint32_t w1d = umma::smem_u32(base + InferSmem::w1);
-      for (uint32_t t = blockIdx.x; t < n_tiles && !failed(); t += gridDim.x) {
-        for (uint32_t j = 0; j < 3 + p.n_chunks && !failed(); ++j, ++J) {
+      bool ok = true;
+      for (uint32_t t = blockIdx.x; ok && t < n_tiles && !failed(); t += gridDim.x) {
+        for (uint32_t j = 0; ok && j < 3 + p.n_chunks && !failed(); ++j, ++J) {
           const uint32_t s = J & 1;
-          // Layers 1-3 and the first W4 chunk wait for their operand rows.
-          if (j <= 3) {
-            if (!umma::mbar_wait(act_ready, A & 1)) { set_err(3); break; }
-            ++A;
-          }
-          if (J >= 2 && !umma::mbar_wait(&acc_empty[s], ((J / 2) + 1) & 1)) { set_err(4); break; }
           uint32_t slot = 0;
           if (j >= 1) {
             slot = G % kRing;
             if (!umma::mbar_wait(&ring_full[slot], (G / kRing) & 1)) { set_err(5); break; }
           }
-          umma::tc_fence_after();
           for (uint32_t h = 0; h < 2; ++h) {
+            // Layers 1-3 and the first W4 chunk wait for this half's operand rows.
+            if (j <= 3) {
+              if (!umma::mbar_wait(&act_ready[h], A[h] & 1)) { set_err(3); ok = false; break; }
+              ++A[h];
+            }
+            if (J >= 2 && !umma::mbar_wait(&acc_empty[s * 2 + h], ((J / 2) + 1) & 1)) {
+              set_err(4);
+              ok = false;
+              break;
+            }
+            umma::tc_fence_after();
             const uint32_t d = tbase + s * 256 + h * 128;
             const uint32_t a = umma::smem_u32(base + InferSmem::act + h * 32768);
             if (j == 0) {
@@ -406,8 +415,9 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
                                idesc, k | acc0);
               }
             }
+            umma::mma_commit(&acc_full[s * 2 + h]);
           }
-          umma::mma_commit(&acc_full[s]);
+          if (!ok) break;
           if (j >= 1) {
             umma::mma_commit(&ring_empty[slot]);
             ++G;
@@ -443,12 +453,12 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
       }
       umma::fence_proxy_async();
       __syncwarp();
-      if (lane == 0) umma::mbar_arrive(act_ready);
+      if (lane == 0) umma::mbar_arrive(&act_ready[h]);
       float best = -INFINITY;
       uint32_t best_idx = 0;
       for (uint32_t j = 0; j < 3 + p.n_chunks; ++j, ++J) {
         const uint32_t s = J & 1;
-        if (!warp_wait(&acc_full[s], (J / 2) & 1)) { set_err(7); break; }
+        if (!warp_wait(&acc_full[s * 2 + h], (J / 2) & 1)) { set_err(7); break; }
         umma::tc_fence_after();
         const uint32_t tcol = tbase + lane_base + s * 256 + h * 128;
         if (j < 3) {
@@ -523,8 +533,8 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
         if (j < 3) umma::fence_proxy_async();
         __syncwarp();
         if (lane == 0) {
-          umma::mbar_arrive(&acc_empty[s]);
-          if (j < 3) umma::mbar_arrive(act_ready);
+          umma::mbar_arrive(&acc_empty[s * 2 + h]);
+          if (j < 3) umma::mbar_arrive(&act_ready[h]);
         }
       }
       if (ray < p.n && !failed()) p.out[ray] = int32_t(best_idx);
