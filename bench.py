@@ -55,9 +55,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="terrain", choices=["terrain", "instanced", "mixture"],
-                    help="terrain: the headline (learned-seeded vs plain nearest, 1M triangles); instanced: "
-                         "two-level frames (refit + mixed launch as a CUDA graph); mixture: D = 6 boxes")
+    ap.add_argument("--workload", default="terrain", choices=["terrain", "boxes", "instanced", "mixture"],
+                    help="terrain: the headline (learned-seeded vs plain nearest, 1M triangles); boxes: 10,000 "
+                         "boxes, 65,536 rays; instanced: two-level frames (refit + mixed launch as a CUDA graph); "
+                         "mixture: D = 6 boxes")
     ap.add_argument("--frames", type=int, default=100, help="instanced: frames timed")
     ap.add_argument("--order", default="near_first", choices=["near_first", "reference"])
     ap.add_argument("--train-rays", type=int, default=1 << 22, help="guide training rays (labelled by plain traversal)")
@@ -318,6 +319,54 @@ def bench_instanced(args):
     ctx.close()
 
 
+def bench_boxes(args):
+    """10,000 axis-aligned boxes (centres U[-100,100]^3, half-extents
+    U[0.25,2]); 65,536 rays from a radius-200 sphere aimed into [-50,50]^3;
+    nearest, t_max 1000, device-resident, with the CPU oracle on all rays."""
+    import torch
+    import spatial_query_b200 as sq
+    from spatial_query_b200 import scenes
+    s = scenes.boxes_scene(seed=0)
+    ctx = sq.Context(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    torch.cuda.set_stream(stream)
+    geom = sq.Geometry("boxes", 3, s["prims"])
+    scene = sq.DeviceBvh(ctx, sq.HostBvh.build(geom), geom)
+    n = s["rays"].shape[0]
+    d_rays = torch.from_numpy(s["rays"]).to(dev)
+    leaf, toi = torch.empty(n, dtype=torch.int32, device=dev), torch.empty(n, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    near = lambda: scene.raycast_nearest_d(d_rays, n, s["max_toi"], leaf, toi)
+    for _ in range(args.warmup):
+        near()
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clk:
+        ms = sum(timed(stream, near, args.steps, flush)) / args.steps
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    sc = O.Scene("boxes", 3, s["prims"])
+    threads = os.cpu_count() or 1
+    sc.nearest(s["rays"][:4096], s["max_toi"], threads=threads)
+    t0 = time.perf_counter()
+    ref = sc.nearest(s["rays"], s["max_toi"], threads=threads)
+    cpu_s = time.perf_counter() - t0
+    same = bool(np.array_equal(ref.leaf, leaf.cpu().numpy().view(np.uint32)))
+    line = {"metric": "Mrays/s nearest-hit, 10,000 boxes, 65,536 rays", "value": round(n / ms / 1000.0, 3),
+            "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded boxes and rays)",
+            "config": {"workload": "10,000 boxes (centres U[-100,100]^3, half-extents U[0.25,2]); 65,536 rays "
+                                   "from a radius-200 sphere toward U[-50,50]^3; t_max 1000",
+                       "identical_to_cpu": same, "l2": "flushed between steps"},
+            "cpu_baseline": {"value": round(n / cpu_s / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
+                             "sample": "all 65,536 rays, one pass"},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    scene.close()
+    ctx.close()
+
+
 def bench_mixture(args):
     """D = 6: 2,097,152 Gaussian-mixture boxes; 1,048,576 nearest rays (t_max
     2) and 262,144 overlap queries (CSR result), device-resident."""
@@ -370,7 +419,7 @@ def main():
         return
     if args.workload != "terrain":
         if rank == 0:
-            (bench_instanced if args.workload == "instanced" else bench_mixture)(args)
+            {"boxes": bench_boxes, "instanced": bench_instanced, "mixture": bench_mixture}[args.workload](args)
         return
 
     import ctypes as C
@@ -439,10 +488,13 @@ def main():
     def seeded():
         guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], g_leaf, g_toi, g_nrm, d_bucket=d_bucket)
 
+    # The autotuner picks the launch configuration (order, blocks per SM) on
+    # these rays; both orders return the reference's hits.
+    tune = scene.autotune_nearest_d(d_rays, n, s["max_toi"], reps=2)
     # Instrumented runs (untimed): counters for the algorithmic bytes, and
     # the identical-hits check.
     st = scene.raycast_nearest_d(d_rays, n, s["max_toi"], d_leaf, d_toi, d_nrm, stats=True)
-    replayed = ctx.last_replay_count if args.order == "near_first" else 0
+    replayed = ctx.last_replay_count
     predict()
     st_g = guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], g_leaf, g_toi, g_nrm, d_bucket=d_bucket,
                                           stats=True)
@@ -495,7 +547,16 @@ def main():
             m = float(t.item())
         return m
 
+    # Config 2's second query: all hits, the first 16 per ray in order, plus full counts.
+    K_ALL = 16
+    a_cnt = torch.empty(n, dtype=torch.int32, device=dev)
+    a_leaf = torch.empty((n, K_ALL), dtype=torch.int32, device=dev)
+    a_toi = torch.empty((n, K_ALL), dtype=torch.float32, device=dev)
+    allhits = lambda: scene.raycast_all_d(d_rays, n, s["max_toi"], K_ALL, a_cnt, a_leaf, a_toi)
+    allhits()
+    al_ms = timed(stream, allhits, args.steps, flush)
     ms, plain_ms, predict_ms, seeded_ms = mean_max(g_ms), mean_max(p_ms), mean_max(pr_ms), mean_max(sd_ms)
+    all_ms = mean_max(al_ms)
     value = world * n / (ms / 1000) / 1e6
     plain_value = world * n / (plain_ms / 1000) / 1e6
 
@@ -571,13 +632,21 @@ def main():
             "vs_baseline": None, "dtype": "f32 (traversal), bf16 x bf16 -> f32 (guide MLP)",
             "data": "synthetic (seeded height field and rays)",
             "config": {"workload": WORKLOAD,
-                       "path": f"learned-seeded: fused tcgen05 MLP inference + seeded {args.order} traversal",
+                       "path": "learned-seeded: fused tcgen05 MLP inference + seeded near-first traversal",
                        "identical_hits": identical,
                        "plain_gpu": {"value": round(plain_value, 3), "unit": "Mrays/s", "ms_per_step": round(plain_ms, 4),
-                                     "path": f"plain GPU traversal, {args.order} order",
+                                     "path": "plain GPU traversal, autotuned: "
+                                             + ("near-first" if tune["best"]["order"] == 0 else "reference order")
+                                             + f", {tune['best']['blocks_per_sm'] or 'occupancy'} blocks per SM",
                                      "e2e_mrays": round(world * n / (e2e_plain_ms / 1000) / 1e6, 3),
                                      "replayed_in_reference_order": int(replayed)},
                        "learned_vs_plain": round(value / plain_value, 4),
+                       "autotune": {"best": tune["best"], "candidates": len(tune["table"]),
+                                    "near_first_best_ms": round(min(e["ms"] for e in tune["table"] if e["order"] == 0), 4),
+                                    "reference_best_ms": round(min(e["ms"] for e in tune["table"] if e["order"] == 1), 4)},
+                       "all_hits_k16": {"value": round(world * n / (all_ms / 1000) / 1e6, 3), "unit": "Mrays/s",
+                                        "ms_per_step": round(all_ms, 4),
+                                        "hits_per_ray": round(float(a_cnt.double().mean().item()), 3)},
                        "breakdown_ms": {"inference": round(predict_ms, 4), "seeded_traversal": round(seeded_ms, 4),
                                         "plain_traversal": round(plain_ms, 4)},
                        "nodes_visited_per_ray": {"plain": round(st["nodes_visited"] / n, 3),

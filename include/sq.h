@@ -54,6 +54,7 @@ extern "C" {
 #define SQ_NARROW_SPHERE 1      /* leaf = centre[D],radius; near root, far root from inside (tests/differential.rs:61-82) */
 #define SQ_NARROW_SPHERE_NEAR 2 /* leaf = centre[D],radius; near root only (tests/gpu.rs:92-106) */
 #define SQ_NARROW_TRIANGLE 3    /* leaf = v0,v1,v2 (D = 3); Moeller-Trumbore (viewport-lib-query/src/lib.rs:295-320) */
+#define SQ_NARROW_CUSTOM 4      /* a consumer narrow phase compiled at run time (sq_bvh_upload_custom) */
 
 /* Traversal order of nearest queries (sq_ctx_set_order). */
 #define SQ_ORDER_NEAR_FIRST 0   /* the default: visit the child with the smaller slab entry first; an answer
@@ -137,6 +138,25 @@ int32_t sq_ctx_set_blocks_per_sm(sq_ctx* ctx, int32_t blocks);
  * slab entry of its own primitive's AABB (the one case where the reference's
  * walk could miss it). */
 int32_t sq_ctx_set_replay_window(sq_ctx* ctx, float window);
+/* Autotuner for nearest rays on one scene: times every candidate launch
+ * configuration on a sample of device-resident rays (CUDA events, best of
+ * `reps`), keeps the fastest in the context and reports the table. The knobs
+ * are the traversal order (near-first, certified / the reference's order,
+ * both give the reference's hits) and the persistent grid's resident blocks
+ * per SM (0 = the occupancy limit). No counterpart in the reference, whose
+ * WGSL path has a fixed 64-thread workgroup (gpu/mod.rs:119-227). */
+typedef struct sq_tune_entry {
+  int32_t order;
+  int32_t blocks_per_sm;
+  float ms;
+} sq_tune_entry;
+typedef struct sq_tune_result {
+  uint32_t n_entries;
+  sq_tune_entry entries[32];
+  int32_t best;  /* index into entries */
+} sq_tune_result;
+int32_t sq_autotune_nearest_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_rays, uint32_t n, float max_toi,
+                              uint32_t reps, sq_tune_result* out);
 /* Kernels this context has launched so far. */
 uint64_t sq_ctx_launch_count(const sq_ctx* ctx);
 /* How many queries of the last near-first launch were answered again, in the
@@ -166,6 +186,27 @@ int32_t sq_bvh_upload(sq_ctx* ctx, int32_t dim, int32_t narrow, uint32_t n_nodes
                       const uint32_t* child_a, const uint32_t* child_b, const uint32_t* prim_count, uint32_t n_prims,
                       const uint32_t* prim_indices, const float* prim_data, uint32_t prim_stride,
                       const uint64_t* layers, const uint32_t* sub_objects, sq_bvh** out);
+
+/* A D = 3 scene whose narrow phase is the caller's own CUDA source, compiled
+ * at upload time with NVRTC into the traversal kernels (the GpuGeometry
+ * contract, gpu/mod.rs:69-99, where the consumer hands a WGSL `narrow`). The
+ * source defines, in the library's namespace (it is wrapped in one):
+ *   __device__ bool sq_narrow(const float* prim, uint32_t leaf, const float* ro,
+ *                             const float* rd, float max_toi, float* toi,
+ *                             float* normal);
+ * prim: the leaf's prim_stride floats (1..32); return true with *toi (not
+ * past max_toi) and normal[3] for a hit. The library's exact maths
+ * (fadd, fmul, ray_at, ...) are in scope. prim_aabbs (min[3], max[3] per
+ * leaf) are the boxes the tree was built from; each must contain its
+ * leaf's hits (near-first answers are certified against them). Ray nearest
+ * and all-hits queries are supported; casts, overlaps and refit return
+ * SQ_ERR_UNSUPPORTED. A source that does not compile returns SQ_ERR_COMPILE
+ * with the compiler log in sq_ctx_last_error. Kernels are cached per source
+ * and stride for the process. */
+int32_t sq_bvh_upload_custom(sq_ctx* ctx, uint32_t n_nodes, const float* node_bounds, const uint32_t* child_a,
+                             const uint32_t* child_b, const uint32_t* prim_count, uint32_t n_prims,
+                             const uint32_t* prim_indices, const float* prim_data, uint32_t prim_stride,
+                             const float* prim_aabbs, const char* narrow_src, sq_bvh** out);
 int32_t sq_bvh_destroy(sq_bvh* bvh);
 int32_t sq_bvh_info_get(const sq_bvh* bvh, sq_bvh_info* out);
 

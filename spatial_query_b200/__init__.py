@@ -100,6 +100,9 @@ SIGNATURES = {
     "sq_ctx_set_replay_window": (C.c_int32, [P, C.c_float]),
     "sq_tree_build": (C.c_int32, [C.c_int32, C.c_uint32, P, C.c_int32, C.c_uint32, P, P, P, P, P, P]),
     "sq_prim_aabbs": (C.c_int32, [C.c_int32, C.c_int32, C.c_uint32, P, P]),
+    "sq_autotune_nearest_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, C.c_uint32, P]),
+    "sq_bvh_upload_custom": (C.c_int32, [P, C.c_uint32, P, P, P, P, C.c_uint32, P, P, C.c_uint32, P, C.c_char_p,
+                                         C.POINTER(P)]),
     "sq_bvh_upload": (C.c_int32, [P, C.c_int32, C.c_int32, C.c_uint32, P, P, P, P, C.c_uint32, P, P, C.c_uint32,
                                   P, P, C.POINTER(P)]),
     "sq_bvh_destroy": (C.c_int32, [P]),
@@ -389,6 +392,14 @@ def _stats_dict(s: _Stats) -> dict:
     return dict(nodes_visited=s.nodes_visited, aabb_tests=s.aabb_tests, narrow_tests=s.narrow_tests, hits=s.hits)
 
 
+class _TuneEntry(C.Structure):
+    _fields_ = [("order", C.c_int32), ("blocks_per_sm", C.c_int32), ("ms", C.c_float)]
+
+
+class _TuneResult(C.Structure):
+    _fields_ = [("n_entries", C.c_uint32), ("entries", _TuneEntry * 32), ("best", C.c_int32)]
+
+
 class DeviceBvh:
     """An uploaded scene: child-pair node records and leaf-ordered primitive
     records in HBM (sq_bvh_upload)."""
@@ -410,6 +421,39 @@ class DeviceBvh:
                                       _p(self._sub), C.byref(h)), "sq_bvh_upload")
         self.h = h
         self.tree = tree
+
+    def autotune_nearest_d(self, d_rays, n, max_toi, reps: int = 3) -> dict:
+        """Times the order x blocks-per-SM candidates on these rays, keeps the
+        fastest in the context (sq_autotune_nearest_d); returns the table."""
+        r = _TuneResult()
+        self.ctx.check(lib().sq_autotune_nearest_d(self.ctx.h, self.h, _p(d_rays), n, float(max_toi), reps,
+                                                   C.byref(r)), "autotune")
+        table = [dict(order=r.entries[i].order, blocks_per_sm=r.entries[i].blocks_per_sm, ms=r.entries[i].ms)
+                 for i in range(r.n_entries)]
+        return dict(best=table[r.best], table=table)
+
+    @classmethod
+    def custom(cls, ctx: Context, tree: HostBvh, prims, aabbs, source: str) -> "DeviceBvh":
+        """A D = 3 scene whose narrow phase is `source` (CUDA defining
+        sq_narrow, compiled at upload with NVRTC; sq_bvh_upload_custom).
+        prims: [n, stride] leaf parameters; aabbs: [n, 6] the boxes the tree
+        was built from."""
+        prims = np.ascontiguousarray(prims, dtype=np.float32)
+        prims = prims.reshape(prims.shape[0], -1)
+        aabbs = np.ascontiguousarray(aabbs, dtype=np.float32).reshape(-1, 6)
+        self = cls.__new__(cls)
+        self.ctx, self.dim, self.geom, self.tree = ctx, 3, None, tree
+        self._layers = self._sub = None
+        h = P()
+        nn = tree.node_count
+        z = np.zeros(4, np.uint32)
+        ctx.check(lib().sq_bvh_upload_custom(ctx.h, nn, _p(tree.bounds if nn else z), _p(tree.child_a if nn else z),
+                                             _p(tree.child_b if nn else z), _p(tree.prim_count if nn else z),
+                                             prims.shape[0], _p(tree.prim_indices if nn else z), _p(prims),
+                                             prims.shape[1], _p(aabbs), source.encode(), C.byref(h)),
+                  "sq_bvh_upload_custom")
+        self.h = h
+        return self
 
     def close(self):
         if getattr(self, "h", None) and _lib is not None:

@@ -30,6 +30,7 @@ UNITS = [
     ("sq_tlas.cu", ["--fmad=false"]),
     ("tlas_kernels.cu", ["--fmad=false"]),
     ("guide.cu", []),
+    ("rtc.cu", ["-I", BUILD]),
     ("tree_build.cpp", []),
 ]
 
@@ -46,8 +47,24 @@ def _deps() -> list[str]:
         os.path.join(HERE, "..", "include", "sq.h")]
 
 
+def write_rtc_sources() -> None:
+    """The traversal headers as string literals, for run-time compilation of
+    consumer narrow phases (rtc.cu): _build/rtc_sources.h."""
+    out = os.path.join(BUILD, "rtc_sources.h")
+    parts = ["// generated by build.py from csrc/sq_math.cuh and csrc/traverse.cuh\n#pragma once\n"]
+    for var, name in (("kRtcMath", "sq_math.cuh"), ("kRtcTraverse", "traverse.cuh")):
+        text = open(os.path.join(CSRC, name)).read()
+        assert ")SQRTC\"" not in text
+        parts.append(f'static const char* const {var} = R"SQRTC({text})SQRTC";\n')
+    new = "".join(parts)
+    if not os.path.exists(out) or open(out).read() != new:
+        with open(out, "w") as f:
+            f.write(new)
+
+
 def build(verbose: bool = False, ptxas_info: bool = False, jobs: int | None = None) -> str:
     os.makedirs(BUILD, exist_ok=True)
+    write_rtc_sources()
     deps = _deps()
     objs = []
     cmds = []
@@ -72,7 +89,8 @@ def build(verbose: bool = False, ptxas_info: bool = False, jobs: int | None = No
             if r.returncode != 0:
                 raise RuntimeError(f"nvcc failed: {cmd[-3]}")
     if cmds or not os.path.exists(LIB):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lpthread"]
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lpthread", "-lnvrtc",
+               "-Xlinker", "-rpath,/usr/local/cuda/lib64"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)

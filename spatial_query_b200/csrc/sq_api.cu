@@ -81,8 +81,9 @@ int32_t nearest_core(sq_ctx* ctx, const sq_bvh* b, bool cast, const float* d_q, 
   const int st = stats ? 1 : 0;
   if (stats && !cast) p.stats = ctx->d_stats;
   const void* ref_fn = cast ? b->ks.cast_nearest[1] : b->ks.ray_nearest[1][st];
-  if (!near_first) return launch_persistent(ctx, ref_fn, p, b->depth, p.n);
   const void* near_fn = cast ? b->ks.cast_nearest[0] : b->ks.ray_nearest[0][st];
+  if (!ref_fn || !near_fn) return fail(ctx, SQ_ERR_UNSUPPORTED, "this scene's narrow phase has no such query");
+  if (!near_first) return launch_persistent(ctx, ref_fn, p, b->depth, p.n);
   return near_first_launch(ctx, b, near_fn, ref_fn, p, b->depth);
 }
 
@@ -114,6 +115,7 @@ int32_t list_core(sq_ctx* ctx, const sq_bvh* b, int kind, const float* d_q, uint
     fn = b->ks.ray_all[stats ? 1 : 0];
     if (stats) p.stats = ctx->d_stats;
   }
+  if (!fn) return fail(ctx, SQ_ERR_UNSUPPORTED, "this scene's narrow phase has no such query");
   return launch_persistent(ctx, fn, p, b->depth, p.n);
 }
 
@@ -244,18 +246,26 @@ extern "C" int32_t sq_ctx_last_replay_count(sq_ctx* ctx, uint32_t* out) {
 // upload / refit
 // ============================================================================
 
-extern "C" int32_t sq_bvh_upload(sq_ctx* ctx, int32_t dim, int32_t narrow, uint32_t n_nodes,
-                                 const float* node_bounds, const uint32_t* child_a, const uint32_t* child_b,
-                                 const uint32_t* prim_count, uint32_t n_prims, const uint32_t* prim_indices,
-                                 const float* prim_data, uint32_t prim_stride, const uint64_t* layers,
-                                 const uint32_t* sub_objects, sq_bvh** out) {
+// The shared upload. A consumer narrow phase (SQ_NARROW_CUSTOM) brings its
+// run-time-compiled kernels in `custom` and the per-leaf AABBs the tree was
+// built from in `prim_aabbs` (stored beside the leaf data).
+static int32_t upload_impl(sq_ctx* ctx, int32_t dim, int32_t narrow, uint32_t n_nodes, const float* node_bounds,
+                           const uint32_t* child_a, const uint32_t* child_b, const uint32_t* prim_count,
+                           uint32_t n_prims, const uint32_t* prim_indices, const float* prim_data,
+                           uint32_t prim_stride, const uint64_t* layers, const uint32_t* sub_objects,
+                           const float* prim_aabbs, const KernelSet* custom, sq_bvh** out) {
   if (!ctx || !out) return SQ_ERR_INVALID;
   *out = nullptr;
   KernelSet ks;
-  if (!kernel_set(dim, narrow, &ks))
-    return fail(ctx, SQ_ERR_UNSUPPORTED, "no kernels for dim " + std::to_string(dim) + " narrow " +
-                                             std::to_string(narrow));
-  if (prim_stride != stride_of(dim, narrow)) return fail(ctx, SQ_ERR_INVALID, "prim_stride does not match the narrow phase");
+  if (custom) {
+    ks = *custom;
+  } else {
+    if (!kernel_set(dim, narrow, &ks))
+      return fail(ctx, SQ_ERR_UNSUPPORTED, "no kernels for dim " + std::to_string(dim) + " narrow " +
+                                               std::to_string(narrow));
+    if (prim_stride != stride_of(dim, narrow))
+      return fail(ctx, SQ_ERR_INVALID, "prim_stride does not match the narrow phase");
+  }
   if (n_prims >= kLeafBit || n_nodes >= kLeafBit) return fail(ctx, SQ_ERR_INVALID, "too many nodes or leaves");
   if ((n_nodes == 0) != (n_prims == 0)) return fail(ctx, SQ_ERR_INVALID, "empty tree with leaves, or leaves without a tree");
   if (n_nodes && (!node_bounds || !child_a || !child_b || !prim_count || !prim_indices || !prim_data))
@@ -269,6 +279,7 @@ extern "C" int32_t sq_bvh_upload(sq_ctx* ctx, int32_t dim, int32_t narrow, uint3
   b->n_nodes = n_nodes;
   b->n_prims = n_prims;
   b->stride = prim_stride;
+  b->prim_vec = custom ? (prim_stride + 2 * dim + 1 + 3) / 4 : prim_vec(dim, narrow);
   b->ks = ks;
   if (n_nodes == 0) {
     *out = b.release();
@@ -324,7 +335,7 @@ extern "C" int32_t sq_bvh_upload(sq_ctx* ctx, int32_t dim, int32_t narrow, uint3
   b->h_count.assign(prim_count, prim_count + n_nodes);
 
   const int D = dim;
-  const uint32_t NV = node_vec(D), PV = prim_vec(D, narrow);
+  const uint32_t NV = node_vec(D), PV = b->prim_vec;
   std::vector<float> nodes(size_t(std::max<uint32_t>(ni, 1)) * NV * 4, 0.f);
   std::vector<uint32_t> parents(std::max<uint32_t>(ni, 1), kNoHit);
   std::vector<RefitLeaf> leaves;
@@ -349,14 +360,20 @@ extern "C" int32_t sq_bvh_upload(sq_ctx* ctx, int32_t dim, int32_t narrow, uint3
 
   // Primitive records in leaf order: payload, then the id (flagged on the
   // last primitive of each leaf).
-  const uint32_t payload = narrow == SQ_NARROW_AABB ? 2 * D : (narrow == SQ_NARROW_TRIANGLE ? 9 : D + 1);
+  const uint32_t payload = custom ? prim_stride + 2 * D
+                                  : (narrow == SQ_NARROW_AABB ? 2 * D : (narrow == SQ_NARROW_TRIANGLE ? 9 : D + 1));
   std::vector<float> prims(size_t(n_prims) * PV * 4, 0.f);
   for (const RefitLeaf& L : leaves) {
     for (uint32_t j = 0; j < L.count; ++j) {
       const uint32_t pos = L.first + j;
       const uint32_t id = prim_indices[pos];
       float* r = prims.data() + size_t(pos) * PV * 4;
-      std::memcpy(r, prim_data + size_t(id) * prim_stride, payload * 4);
+      if (custom) {
+        std::memcpy(r, prim_data + size_t(id) * prim_stride, prim_stride * 4);
+        std::memcpy(r + prim_stride, prim_aabbs + size_t(id) * 2 * D, 2 * D * 4);
+      } else {
+        std::memcpy(r, prim_data + size_t(id) * prim_stride, payload * 4);
+      }
       uint32_t w = id | (j + 1 == L.count ? kLeafBit : 0u);
       std::memcpy(&r[payload], &w, 4);
     }
@@ -390,6 +407,36 @@ extern "C" int32_t sq_bvh_upload(sq_ctx* ctx, int32_t dim, int32_t narrow, uint3
   return SQ_OK;
 }
 
+extern "C" int32_t sq_bvh_upload(sq_ctx* ctx, int32_t dim, int32_t narrow, uint32_t n_nodes,
+                                 const float* node_bounds, const uint32_t* child_a, const uint32_t* child_b,
+                                 const uint32_t* prim_count, uint32_t n_prims, const uint32_t* prim_indices,
+                                 const float* prim_data, uint32_t prim_stride, const uint64_t* layers,
+                                 const uint32_t* sub_objects, sq_bvh** out) {
+  if (narrow == SQ_NARROW_CUSTOM) return fail(ctx, SQ_ERR_INVALID, "a consumer narrow phase uploads through sq_bvh_upload_custom");
+  return upload_impl(ctx, dim, narrow, n_nodes, node_bounds, child_a, child_b, prim_count, n_prims, prim_indices,
+                     prim_data, prim_stride, layers, sub_objects, nullptr, nullptr, out);
+}
+
+extern "C" int32_t sq_bvh_upload_custom(sq_ctx* ctx, uint32_t n_nodes, const float* node_bounds,
+                                        const uint32_t* child_a, const uint32_t* child_b, const uint32_t* prim_count,
+                                        uint32_t n_prims, const uint32_t* prim_indices, const float* prim_data,
+                                        uint32_t prim_stride, const float* prim_aabbs, const char* narrow_src,
+                                        sq_bvh** out) {
+  if (!ctx || !out) return SQ_ERR_INVALID;
+  *out = nullptr;
+  if (!narrow_src) return fail(ctx, SQ_ERR_INVALID, "null narrow-phase source");
+  if (prim_stride == 0 || prim_stride > kMaxCustomStride)
+    return fail(ctx, SQ_ERR_INVALID, "prim_stride must be 1.." + std::to_string(kMaxCustomStride));
+  if (n_prims && (!prim_aabbs || !prim_data)) return fail(ctx, SQ_ERR_INVALID, "null primitive data or AABBs");
+  KernelSet ks;
+  std::string log;
+  CK(cudaSetDevice(ctx->device));
+  const int32_t rc = rtc_kernel_set(prim_stride, narrow_src, &ks, &log);
+  if (rc != SQ_OK) return fail(ctx, rc, log);
+  return upload_impl(ctx, 3, SQ_NARROW_CUSTOM, n_nodes, node_bounds, child_a, child_b, prim_count, n_prims,
+                     prim_indices, prim_data, prim_stride, nullptr, nullptr, prim_aabbs, &ks, out);
+}
+
 extern "C" int32_t sq_bvh_destroy(sq_bvh* b) {
   if (!b) return SQ_OK;
   cudaSetDevice(b->device);
@@ -411,7 +458,7 @@ extern "C" int32_t sq_bvh_info_get(const sq_bvh* b, sq_bvh_info* o) {
   o->n_interior = b->n_interior;
   o->device_bytes = b->bytes;
   o->node_record_bytes = node_vec(b->dim) * 16;
-  o->prim_record_bytes = prim_vec(b->dim, b->narrow) * 16;
+  o->prim_record_bytes = b->prim_vec * 16;
   return SQ_OK;
 }
 
@@ -420,6 +467,7 @@ extern "C" int32_t sq_bvh_refit_d(sq_ctx* ctx, sq_bvh* b, const float* d_prim_da
   if (rc) return rc;
   if (b->n_nodes == 0) return SQ_OK;
   if (!d_prim_data) return fail(ctx, SQ_ERR_INVALID, "null prim data");
+  if (!b->ks.refit_leaves) return fail(ctx, SQ_ERR_UNSUPPORTED, "this scene's narrow phase has no refit");
   CK(cudaMemsetAsync(b->d_arrivals, 0, size_t(std::max<uint32_t>(b->n_interior, 1)) * 4, ctx->stream));
   CK(cudaMemsetAsync(b->d_nonfinite, 0, sizeof(int), ctx->stream));
   RefitParams p;
@@ -546,6 +594,7 @@ size_t overlap_scan_temp(uint32_t n) {
 int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint32_t n, const sq_filter* f,
                      uint64_t* d_offsets, uint32_t* d_leaves, uint64_t cap, uint64_t* total, void* scratch,
                      size_t scratch_bytes) {
+  if (!b->ks.overlap) return fail(ctx, SQ_ERR_UNSUPPORTED, "this scene's narrow phase has no overlap query");
   uint32_t* d_counts = (uint32_t*)scratch;
   size_t counts_bytes = ((size_t(n) + 1) * 4 + 255) & ~size_t(255);
   void* temp = (char*)scratch + counts_bytes;
@@ -858,6 +907,7 @@ extern "C" int32_t sq_overlap_noalloc(const sq_bvh* b, const float* d_regions, u
                                       uint64_t* total, void* stream) {
   if (!b || !d_offsets || !total || (n && !d_regions)) return SQ_ERR_INVALID;
   if (n > kNoAllocMaxRegions) return SQ_ERR_CAPACITY;  // beyond the static scratch
+  if (!b->ks.overlap) return SQ_ERR_UNSUPPORTED;
   NoAllocDevice* d = nullptr;
   int32_t rc = noalloc_setup(b->device, b->ks.overlap, &d);
   if (rc) return rc;
@@ -956,7 +1006,6 @@ int32_t sqi::seeded_nearest(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, u
 
 int32_t sqi::near_first_launch(sq_ctx* ctx, const sq_bvh* b, const void* fn, const void* ref_fn, QueryParams& p,
                                uint32_t stack) {
-  (void)b;
   // The replay list holds at most every query of the batch; it grows here,
   // outside any stream capture once a batch of this size has run.
   const size_t need = size_t(std::max<uint32_t>(p.n, 1)) * sizeof(uint32_t);
@@ -974,6 +1023,9 @@ int32_t sqi::near_first_launch(sq_ctx* ctx, const sq_bvh* b, const void* fn, con
   p.window = ctx->window;
   int32_t rc = launch_persistent(ctx, fn, p, stack, p.n);
   if (rc) return rc;
+  // A box leaf's hit is its own slab entry, so box answers are always
+  // certified and nothing is ever appended: no replay launch.
+  if (b->narrow == SQ_NARROW_AABB) return SQ_OK;
   // The uncertified queries again, in the reference order, unseeded.
   QueryParams r = p;
   r.replay_count = nullptr;
@@ -982,4 +1034,70 @@ int32_t sqi::near_first_launch(sq_ctx* ctx, const sq_bvh* b, const void* fn, con
   r.q_list = static_cast<const uint32_t*>(ctx->replay_list.p);
   r.q_count = ctx->d_replays;
   return launch_persistent(ctx, ref_fn, r, b->depth, p.n);
+}
+
+// ============================================================================
+// autotuner (include/sq.h)
+// ============================================================================
+
+extern "C" int32_t sq_autotune_nearest_d(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, uint32_t n, float max_toi,
+                                         uint32_t reps, sq_tune_result* out) {
+  int32_t rc = check_scene(ctx, b);
+  if (rc) return rc;
+  if (!out || !d_rays || n == 0) return fail(ctx, SQ_ERR_INVALID, "autotune needs rays and a result");
+  std::memset(out, 0, sizeof(*out));
+  reps = std::max<uint32_t>(reps, 1);
+  uint32_t* d_leaf = nullptr;
+  float* d_toi = nullptr;
+  if ((rc = arena_reserve(ctx, size_t(n) * 8 + 512))) return rc;
+  d_leaf = static_cast<uint32_t*>(ctx->arena.p);
+  d_toi = reinterpret_cast<float*>(static_cast<char*>(ctx->arena.p) + ((size_t(n) * 4 + 255) & ~size_t(255)));
+  sq_hits o{};
+  o.leaf = d_leaf;
+  o.toi = d_toi;
+  const int saved_order = ctx->order, saved_bps = ctx->blocks_per_sm;
+  const int orders[2] = {SQ_ORDER_NEAR_FIRST, SQ_ORDER_REFERENCE};
+  const int bps[8] = {0, 2, 4, 6, 8, 10, 12, 16};
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best = 0.f;
+  for (int oi = 0; oi < 2 && rc == SQ_OK; ++oi) {
+    for (int bi = 0; bi < 8 && rc == SQ_OK; ++bi) {
+      ctx->order = orders[oi];
+      ctx->blocks_per_sm = bps[bi];
+      // warm, then the best of `reps`
+      if ((rc = nearest_core(ctx, b, false, d_rays, n, max_toi, nullptr, nullptr, o, false))) break;
+      float t_best = 0.f;
+      for (uint32_t r = 0; r < reps; ++r) {
+        CK(cudaEventRecord(e0, ctx->stream));
+        if ((rc = nearest_core(ctx, b, false, d_rays, n, max_toi, nullptr, nullptr, o, false))) break;
+        CK(cudaEventRecord(e1, ctx->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (r == 0 || ms < t_best) t_best = ms;
+      }
+      if (rc) break;
+      sq_tune_entry& e = out->entries[out->n_entries];
+      e.order = orders[oi];
+      e.blocks_per_sm = bps[bi];
+      e.ms = t_best;
+      if (out->n_entries == 0 || t_best < best) {
+        best = t_best;
+        out->best = int32_t(out->n_entries);
+      }
+      ++out->n_entries;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) {
+    ctx->order = saved_order;
+    ctx->blocks_per_sm = saved_bps;
+    return rc;
+  }
+  ctx->order = out->entries[out->best].order;
+  ctx->blocks_per_sm = out->entries[out->best].blocks_per_sm;
+  return finish(ctx);
 }

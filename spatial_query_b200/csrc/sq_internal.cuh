@@ -60,6 +60,7 @@ struct sq_bvh {
   int narrow = 0;
   uint32_t n_nodes = 0, n_prims = 0, n_interior = 0, depth = 0, n_leaves = 0;
   uint32_t stride = 0;
+  uint32_t prim_vec = 0;  // 16-byte vectors per primitive record
   uint32_t root_code = 0;
   float4* d_nodes = nullptr;
   float4* d_prims = nullptr;
@@ -86,6 +87,12 @@ using namespace sq;
 // the queries it could not certify (sq_api.cu).
 int32_t near_first_launch(sq_ctx* ctx, const sq_bvh* b, const void* fn, const void* ref_fn, QueryParams& p,
                           uint32_t stack);
+
+// Consumer narrow phases (rtc.cpp): the kernels of a D = 3 scene whose
+// narrow phase is `src` with `stride` floats per leaf, compiled with NVRTC
+// (cached per stride and source). SQ_ERR_COMPILE with the compiler log.
+constexpr uint32_t kMaxCustomStride = 32;
+int32_t rtc_kernel_set(uint32_t stride, const char* src, KernelSet* out, std::string* log);
 
 // Learned-seeded nearest rays (sq_api.cu): enqueues the SEED kernel.
 int32_t seeded_nearest(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, uint32_t n, float max_toi,

@@ -8,7 +8,15 @@
 // correctly rounded IEEE forms.
 #pragma once
 
+#ifdef __CUDACC_RTC__
+// Runtime compilation (NVRTC, for consumer narrow phases) has no <cstdint>.
+typedef unsigned int uint32_t;
+typedef int int32_t;
+typedef unsigned long long uint64_t;
+typedef long long int64_t;
+#else
 #include <cstdint>
+#endif
 
 namespace sq {
 

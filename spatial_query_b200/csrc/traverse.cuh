@@ -24,7 +24,22 @@
 
 namespace sq {
 
-enum Narrow : int { kNarrowAabb = 0, kNarrowSphere = 1, kNarrowSphereNear = 2, kNarrowTri = 3 };
+enum Narrow : int { kNarrowAabb = 0, kNarrowSphere = 1, kNarrowSphereNear = 2, kNarrowTri = 3, kNarrowCustom = 4 };
+
+// A consumer narrow phase (kNarrowCustom) is compiled at run time with NVRTC
+// into the same kernels: its source defines
+//   __device__ bool sq_narrow(const float* prim, uint32_t leaf, const float* ro, const float* rd,
+//                             float max_toi, float* toi, float* normal);
+// and SQ_CUSTOM_STRIDE is the number of floats per leaf. Its primitive
+// record holds those floats, then the leaf's AABB (the box the tree was built
+// from, used to certify near-first answers), then the id word.
+#ifndef SQ_CUSTOM_STRIDE
+#define SQ_CUSTOM_STRIDE 1
+#endif
+#ifdef SQ_RTC_CUSTOM
+__device__ bool sq_narrow(const float* prim, uint32_t leaf, const float* ro, const float* rd, float max_toi, float* toi,
+                          float* normal);
+#endif
 enum QKind : int { kRayNearest = 0, kRayAll = 1, kCastNearest = 2, kCastAll = 3, kOverlap = 4 };
 
 constexpr int kThreads = 128;
@@ -36,7 +51,10 @@ template <int D> struct NodeLayout {
 };
 
 template <int D, int N> struct PrimLayout {
-  static constexpr int payload = (N == kNarrowAabb) ? 2 * D : (N == kNarrowTri ? 9 : D + 1);
+  static constexpr int payload = (N == kNarrowAabb)     ? 2 * D
+                                 : (N == kNarrowTri)    ? 9
+                                 : (N == kNarrowCustom) ? SQ_CUSTOM_STRIDE + 2 * D
+                                                        : D + 1;
   static constexpr int id_word = payload;
   static constexpr int vec = (payload + 1 + 3) / 4;
 };
@@ -127,6 +145,12 @@ __device__ __forceinline__ float prim_entry(const float* rec, const RayPre<D>& r
   const float inf = __int_as_float(0x7f800000);
   if constexpr (N == kNarrowTri) {
     tri_aabb(rec, rec + 3, rec + 6, lo, hi);
+  } else if constexpr (N == kNarrowCustom) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      lo[i] = rec[SQ_CUSTOM_STRIDE + i];
+      hi[i] = rec[SQ_CUSTOM_STRIDE + D + i];
+    }
   } else if constexpr (N == kNarrowSphere || N == kNarrowSphereNear) {
 #pragma unroll
     for (int i = 0; i < D; ++i) {
@@ -160,6 +184,14 @@ __device__ __forceinline__ bool narrow_ray(const float* rec, const RayPre<D>& r,
     return true;
   } else if constexpr (N == kNarrowSphere || N == kNarrowSphereNear) {
     return ray_ball<D, N == kNarrowSphere>(r.o, r.d, rec, rec[D], max_toi, t, n);
+  } else if constexpr (N == kNarrowCustom) {
+#ifdef SQ_RTC_CUSTOM
+    const uint32_t leaf = __float_as_uint(rec[PrimLayout<D, N>::id_word]) & ~kLeafBit;
+    if (!sq_narrow(rec, leaf, r.o, r.d, max_toi, &t, n)) return false;
+    return !(t > max_toi);
+#else
+    return false;
+#endif
   } else {
     if (!ray_triangle(r.o, r.d, rec, rec + 3, rec + 6, t)) return false;
     if (t > max_toi) return false;
@@ -754,6 +786,7 @@ struct KernelSet {
   const void* ray_nearest_seeded[2];  // [stats]; D = 3 only
 };
 
+#ifndef __CUDACC_RTC__  // host code: not part of a run-time compiled unit
 template <int D, int N> KernelSet make_kernel_set() {
   KernelSet s;
   s.ray_nearest[0][0] = (const void*)query_kernel<D, N, kRayNearest, false, false>;
@@ -775,5 +808,6 @@ template <int D, int N> KernelSet make_kernel_set() {
   }
   return s;
 }
+#endif
 
 }  // namespace sq
