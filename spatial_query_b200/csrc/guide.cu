@@ -300,6 +300,17 @@ struct InferSmem {
   static constexpr uint32_t bytes = bars + 256 + 1024;
 };
 
+// A logit with the index i (0..127) of its column in the low 7 mantissa bits,
+// as 127 - i: (x | 0x7F) ^ i. Written as one LOP3 whose mask comes from a
+// register the compiler cannot fold (r7f is read from shared memory), so i
+// is the instruction's only immediate: one ALU operation per logit, where
+// the two-immediate form costs two.
+__device__ __forceinline__ float tag7(float x, uint32_t r7f, uint32_t i) {
+  uint32_t r;
+  asm("lop3.b32 %0, %1, %2, %3, 0x56;" : "=r"(r) : "r"(__float_as_uint(x)), "r"(r7f), "r"(i));
+  return __uint_as_float(r);
+}
+
 __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const InferParams p) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = umma::smem_u32(smem_raw);
@@ -317,6 +328,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
   uint64_t* fin = bars + 17;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 18);
   int* s_err = reinterpret_cast<int*>(bars + 19);
+  uint32_t* s_r7f = reinterpret_cast<uint32_t*>(bars + 20);  // 0x7F, for tag7
   const float* s_bias = reinterpret_cast<const float*>(base + InferSmem::bias);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -338,6 +350,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
     umma::mbar_init(&act_ready[1], 4);
     umma::mbar_init(fin, 1);
     *s_err = 0;
+    *s_r7f = 0x7Fu;
     umma::fence_barrier_init();
   }
   __syncwarp();
@@ -488,16 +501,15 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
           const uint32_t c0 = (j - 3) * 128;
           float m = -INFINITY;
           const bool full = c0 + 128 <= p.n_buckets;
+          const uint32_t r7f = *reinterpret_cast<volatile uint32_t*>(s_r7f);
           float v[128];
           umma::tmem_ld128(tcol, v);  // the chunk's 128 logits of this row in one load and one wait
           if (full) {
             float m1 = -INFINITY;  // two independent max chains
 #pragma unroll
             for (uint32_t i = 0; i < 128; i += 4) {
-              const float k0 = __uint_as_float((__float_as_uint(v[i]) & 0xFFFFFF80u) | (127u - i));
-              const float k1 = __uint_as_float((__float_as_uint(v[i + 1]) & 0xFFFFFF80u) | (126u - i));
-              const float k2 = __uint_as_float((__float_as_uint(v[i + 2]) & 0xFFFFFF80u) | (125u - i));
-              const float k3 = __uint_as_float((__float_as_uint(v[i + 3]) & 0xFFFFFF80u) | (124u - i));
+              const float k0 = tag7(v[i], r7f, i), k1 = tag7(v[i + 1], r7f, i + 1);
+              const float k2 = tag7(v[i + 2], r7f, i + 2), k3 = tag7(v[i + 3], r7f, i + 3);
               m = umma::fmax3(m, k0, k1);
               m1 = umma::fmax3(m1, k2, k3);
             }
@@ -506,7 +518,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
 #pragma unroll
             for (uint32_t i = 0; i < 128; ++i) {
               const float l = (c0 + i < p.n_buckets) ? v[i] : -INFINITY;
-              m = fmaxf(m, __uint_as_float((__float_as_uint(l) & 0xFFFFFF80u) | (127u - i)));
+              m = fmaxf(m, tag7(l, r7f, i));
             }
           }
           if (m > best) {

@@ -88,11 +88,18 @@ def test_gradients_match_cpu(ctx):
         assert err <= 2e-2, (k, err)
 
 
-def test_inference_matches_cpu_argmax(ctx):
-    s, geom, tree = small_terrain()
+@pytest.mark.parametrize("grid", ["full", "ragged"])
+def test_inference_matches_cpu_argmax(ctx, grid):
+    if grid == "full":  # 4,096 buckets, fewer tiles than CTAs
+        s, geom, tree = small_terrain()
+    else:  # a few hundred buckets (a partial output chunk), several tiles per CTA
+        s = scenes.terrain_scene(seed=6, nx=20, ny=18, n_coherent=20000, n_incoherent=20000)
+        geom = sq.Geometry("tris", 3, s["prims"])
+        tree = sq.HostBvh.build(geom)
     scene = sq.DeviceBvh(ctx, tree, geom)
     guide = sq.Guide(scene, depth=12, batch=256, seed=9)
     info = guide.info()
+    assert info["n_out"] % 128 == 0 and info["n_buckets"] <= info["n_out"] < info["n_buckets"] + 128
     rays = s["rays"]
     n = rays.shape[0] - 37  # a ragged last tile
     d_rays = torch.from_numpy(rays[:n].copy()).to(DEV)
