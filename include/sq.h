@@ -173,6 +173,17 @@ int32_t sq_tree_build(int32_t dim, uint32_t n, const float* prim_aabbs, int32_t 
                       uint32_t* n_nodes_out, float* node_bounds, uint32_t* child_a, uint32_t* child_b,
                       uint32_t* prim_count, uint32_t* prim_indices);
 
+/* The same tree built on the device: d_prim_aabbs and every output are device
+ * pointers (same layouts and capacity rule as sq_tree_build), the arrays equal
+ * sq_tree_build's (bounds compare equal; a zero bound may differ in sign,
+ * which f32::min / max leave unspecified). Runs on the context's stream and
+ * returns once the tree is complete; *n_nodes_out is the node count. A
+ * per-frame rebuild (Tlas::needs_rebuild, accel/tlas.rs:58-60) no longer
+ * needs the host. */
+int32_t sq_tree_build_d(sq_ctx* ctx, int32_t dim, uint32_t n, const float* d_prim_aabbs, uint32_t node_capacity,
+                        uint32_t* n_nodes_out, float* d_node_bounds, uint32_t* d_child_a, uint32_t* d_child_b,
+                        uint32_t* d_prim_count, uint32_t* d_prim_indices);
+
 /* The world AABB of each built-in leaf (the providers' world_aabb). */
 int32_t sq_prim_aabbs(int32_t dim, int32_t narrow, uint32_t n, const float* prim_data, float* out_aabbs);
 

@@ -100,6 +100,7 @@ SIGNATURES = {
     "sq_ctx_set_replay_window": (C.c_int32, [P, C.c_float]),
     "sq_tree_build": (C.c_int32, [C.c_int32, C.c_uint32, P, C.c_int32, C.c_uint32, P, P, P, P, P, P]),
     "sq_prim_aabbs": (C.c_int32, [C.c_int32, C.c_int32, C.c_uint32, P, P]),
+    "sq_tree_build_d": (C.c_int32, [P, C.c_int32, C.c_uint32, P, C.c_uint32, P, P, P, P, P, P]),
     "sq_autotune_nearest_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, C.c_uint32, P]),
     "sq_bvh_upload_custom": (C.c_int32, [P, C.c_uint32, P, P, P, P, C.c_uint32, P, P, C.c_uint32, P, C.c_char_p,
                                          C.POINTER(P)]),
@@ -269,6 +270,39 @@ class HostBvh:
     @classmethod
     def build(cls, geom: Geometry, threads: int = 0) -> "HostBvh":
         return cls.build_from_aabbs(geom.dim, geom.world_aabbs(), threads)
+
+    @classmethod
+    def build_on_device(cls, ctx: "Context", dim: int, aabbs: np.ndarray) -> "HostBvh":
+        """The same tree built on the GPU (sq_tree_build_d), read back."""
+        import torch
+        aabbs = _f32(aabbs).reshape(-1, 2 * dim)
+        n = aabbs.shape[0]
+        dev = torch.device("cuda", ctx.device)
+        d_aabbs = torch.from_numpy(aabbs).to(dev)
+        arrays = tree_build_d(ctx, dim, d_aabbs, n)
+        torch.cuda.synchronize(dev)
+        b, ca, cb, pc, pi = (t.cpu().numpy() for t in arrays)
+        u = lambda a: a.view(np.uint32)
+        return cls(dim, b, u(ca), u(cb), u(pc), u(pi))
+
+
+def tree_build_d(ctx: "Context", dim: int, d_aabbs, n: int):
+    """sq_tree_build_d on device AABBs (a CUDA tensor of n x 2*dim floats):
+    (node_bounds, child_a, child_b, prim_count, prim_indices) as CUDA tensors
+    cut to the node count (int32 tensors hold the u32 fields)."""
+    import torch
+    dev = d_aabbs.device
+    cap = max(2 * n - 1, 1)
+    b = torch.empty((cap, 2 * dim), dtype=torch.float32, device=dev)
+    ca, cb, pc = (torch.empty(cap, dtype=torch.int32, device=dev) for _ in range(3))
+    pi = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    torch.cuda.synchronize(dev)
+    nn = C.c_uint32(0)
+    ctx.check(lib().sq_tree_build_d(ctx.h, dim, n, C.c_void_p(d_aabbs.data_ptr()), cap, C.byref(nn),
+                                    C.c_void_p(b.data_ptr()), C.c_void_p(ca.data_ptr()), C.c_void_p(cb.data_ptr()),
+                                    C.c_void_p(pc.data_ptr()), C.c_void_p(pi.data_ptr())), "sq_tree_build_d")
+    k = nn.value
+    return b[:k], ca[:k], cb[:k], pc[:k], pi[:n]
 
 
 # ---------------------------------------------------------------------------

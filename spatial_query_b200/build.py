@@ -30,6 +30,7 @@ UNITS = [
     ("sq_tlas.cu", ["--fmad=false"]),
     ("tlas_kernels.cu", ["--fmad=false"]),
     ("guide.cu", []),
+    ("tree_build_gpu.cu", ["--fmad=false"]),
     ("rtc.cu", ["-I", BUILD]),
     ("tree_build.cpp", []),
 ]

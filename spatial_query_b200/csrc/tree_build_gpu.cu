@@ -1,0 +1,348 @@
+// Device build of the crate's median-split tree: tree::build
+// (crates/spatial-query/src/accel/tree.rs:39-49, 112-163) on the GPU. The
+// output is the host restatement's (sq_tree_build, tree_build.cpp) array for
+// array: preorder nodes with the root at 0; a leaf holds <= 4 primitives
+// unless all its centroids coincide within f32::EPSILON on the longest
+// centroid axis; the split axis is the first longest axis of the centroid
+// bounds; the primitives of a node are stably sorted by that centroid
+// coordinate under f32::total_cmp and split at start + count / 2.
+//
+// How: the recursion runs a level at a time. For every segment of a level
+// (a node's range of the primitive order), one group of threads reduces the
+// node's box and its centroid box, decides leaf or split, and writes the sort
+// key of each of its primitives; one segmented stable sort then orders every
+// split segment of the level at once, which is the per-node stable sort of
+// the crate (ties keep the order the parent's sort left). Nodes are numbered
+// in level order as they are made; preorder numbers follow from subtree sizes
+// (bottom-up, a level at a time) and left-subtree offsets (top-down).
+#include <cub/device/device_segmented_sort.cuh>
+
+#include <algorithm>
+#include <vector>
+
+#include "sq_internal.cuh"
+
+using sqi::cuda_fail;
+
+namespace {
+
+constexpr uint32_t kLeafSize = 4;
+constexpr float kEps = 1.1920928955078125e-7f;  // f32::EPSILON
+constexpr int kMaxDim = 8;
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+
+struct Seg {
+  uint32_t s, e, node;  // positions [s, e) of the primitive order; level-order node id
+};
+
+struct LNode {
+  uint32_t s, e, a, b;  // range; children's level-order ids (a == kNone: leaf)
+};
+
+// f32::total_cmp as an unsigned order: negative values bit-inverted,
+// non-negative values with the sign bit set.
+__device__ __forceinline__ uint32_t total_ukey(float x) {
+  const uint32_t b = __float_as_uint(x);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+// Aabb::center (aabb.rs:56-58): (min + max) * 0.5 per axis.
+__device__ __forceinline__ float centre(const float* box, int D, int k) {
+  return __fmul_rn(__fadd_rn(box[k], box[D + k]), 0.5f);
+}
+
+__global__ void keys_kernel(const float* __restrict__ aabbs, uint32_t n, int D, uint32_t* keys, uint32_t* idx) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    idx[i] = i;
+    const float* b = aabbs + size_t(i) * 2 * D;
+    for (int k = 0; k < D; ++k) keys[size_t(k) * n + i] = total_ukey(centre(b, D, k));
+  }
+}
+
+struct LevelParams {
+  const float* aabbs;
+  int D;
+  uint32_t n;
+  const uint32_t* keys;  // [D][n]
+  const uint32_t* idx;   // the current primitive order
+  const Seg* cur;
+  uint32_t m;            // segments of this level
+  Seg* next;             // the next level's segments (appended)
+  uint32_t* counters;    // [0] next segments, [1] nodes made, [2] sort segments
+  LNode* nodes;          // by level-order id
+  float* bounds;         // by level-order id: min[D], max[D]
+  uint32_t* sort_beg;
+  uint32_t* sort_end;
+  uint32_t* sort_keys;   // per position: the key of its segment's split axis
+};
+
+// One group of TPS threads per segment (TPS = 32: a warp; TPS = blockDim:
+// the whole block, for the few large segments of the top levels).
+template <int TPS>
+__global__ void __launch_bounds__(256) level_kernel(const LevelParams p) {
+  const uint32_t groups = blockDim.x / TPS;
+  const uint32_t g = blockIdx.x * groups + threadIdx.x / TPS;
+  const uint32_t lane = threadIdx.x % TPS;
+  if (g >= p.m) return;  // uniform per group (and per block when TPS == blockDim)
+  const int D = p.D;
+  const Seg sg = p.cur[g];
+  float lo[kMaxDim], hi[kMaxDim], clo[kMaxDim], chi[kMaxDim];
+#pragma unroll
+  for (int k = 0; k < kMaxDim; ++k) {
+    lo[k] = clo[k] = INFINITY;
+    hi[k] = chi[k] = -INFINITY;
+  }
+  for (uint32_t pos = sg.s + lane; pos < sg.e; pos += TPS) {
+    const float* b = p.aabbs + size_t(p.idx[pos]) * 2 * D;
+#pragma unroll
+    for (int k = 0; k < kMaxDim; ++k) {
+      if (k < D) {
+        lo[k] = fminf(lo[k], b[k]);
+        hi[k] = fmaxf(hi[k], b[D + k]);
+        const float c = centre(b, D, k);
+        clo[k] = fminf(clo[k], c);
+        chi[k] = fmaxf(chi[k], c);
+      }
+    }
+  }
+  // Group reduction (min / max are exact in any order).
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int k = 0; k < kMaxDim; ++k) {
+      if (k < D) {
+        lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+        hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+        clo[k] = fminf(clo[k], __shfl_xor_sync(0xffffffffu, clo[k], o));
+        chi[k] = fmaxf(chi[k], __shfl_xor_sync(0xffffffffu, chi[k], o));
+      }
+    }
+  }
+  __shared__ float red[8][4 * kMaxDim];
+  __shared__ int s_axis;
+  if constexpr (TPS > 32) {
+    const uint32_t w = threadIdx.x / 32;
+    if ((threadIdx.x & 31) == 0) {
+      for (int k = 0; k < D; ++k) {
+        red[w][k] = lo[k];
+        red[w][kMaxDim + k] = hi[k];
+        red[w][2 * kMaxDim + k] = clo[k];
+        red[w][3 * kMaxDim + k] = chi[k];
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (uint32_t v = 1; v < TPS / 32; ++v) {
+        for (int k = 0; k < D; ++k) {
+          lo[k] = fminf(lo[k], red[v][k]);
+          hi[k] = fmaxf(hi[k], red[v][kMaxDim + k]);
+          clo[k] = fminf(clo[k], red[v][2 * kMaxDim + k]);
+          chi[k] = fmaxf(chi[k], red[v][3 * kMaxDim + k]);
+        }
+      }
+    }
+  }
+  // Leaf or split (tree.rs:129-154), decided by the group's first thread.
+  int axis = -1;
+  if (lane == 0) {
+    const uint32_t count = sg.e - sg.s;
+    float* bo = p.bounds + size_t(sg.node) * 2 * D;
+    for (int k = 0; k < D; ++k) {
+      bo[k] = lo[k];
+      bo[D + k] = hi[k];
+    }
+    LNode nd{sg.s, sg.e, kNone, kNone};
+    if (count > kLeafSize) {
+      int ax = 0;
+      float ext[kMaxDim];
+      for (int k = 0; k < D; ++k) ext[k] = __fsub_rn(chi[k], clo[k]);
+      for (int k = 1; k < D; ++k)
+        if (ext[k] > ext[ax]) ax = k;
+      if (ext[ax] > kEps) {
+        axis = ax;
+        const uint32_t mid = sg.s + count / 2;
+        const uint32_t c0 = atomicAdd(&p.counters[0], 2u);
+        const uint32_t id0 = atomicAdd(&p.counters[1], 2u);
+        p.next[c0] = Seg{sg.s, mid, id0};
+        p.next[c0 + 1] = Seg{mid, sg.e, id0 + 1};
+        nd.a = id0;
+        nd.b = id0 + 1;
+        const uint32_t q = atomicAdd(&p.counters[2], 1u);
+        p.sort_beg[q] = sg.s;
+        p.sort_end[q] = sg.e;
+      }
+    }
+    p.nodes[sg.node] = nd;
+  }
+  if constexpr (TPS > 32) {
+    if (threadIdx.x == 0) s_axis = axis;
+    __syncthreads();
+    axis = s_axis;
+  } else {
+    axis = __shfl_sync(0xffffffffu, axis, 0);
+  }
+  if (axis < 0) return;
+  const uint32_t* key = p.keys + size_t(axis) * p.n;
+  for (uint32_t pos = sg.s + lane; pos < sg.e; pos += TPS) p.sort_keys[pos] = key[p.idx[pos]];
+}
+
+// Subtree node counts, one level at a time from the deepest.
+__global__ void sizes_kernel(const LNode* __restrict__ nodes, uint32_t lb, uint32_t le, uint32_t* size) {
+  const uint32_t id = lb + blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= le) return;
+  const LNode nd = nodes[id];
+  size[id] = nd.a == kNone ? 1u : 1u + size[nd.a] + size[nd.b];
+}
+
+// Preorder numbers, one level at a time from the root: the left child
+// follows its parent, the right child follows the left subtree.
+__global__ void preorder_kernel(const LNode* __restrict__ nodes, uint32_t lb, uint32_t le, const uint32_t* size,
+                                uint32_t* pre) {
+  const uint32_t id = lb + blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= le) return;
+  const LNode nd = nodes[id];
+  if (nd.a == kNone) return;
+  pre[nd.a] = pre[id] + 1;
+  pre[nd.b] = pre[id] + 1 + size[nd.a];
+}
+
+// The crate's node arrays in preorder (tree::Node: bounds, and either the
+// children's indices or the leaf's first position and count).
+__global__ void emit_kernel(const LNode* __restrict__ nodes, const float* __restrict__ lbounds,
+                            const uint32_t* __restrict__ pre, uint32_t n_nodes, int D, float* node_bounds,
+                            uint32_t* child_a, uint32_t* child_b, uint32_t* prim_count) {
+  const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= n_nodes) return;
+  const LNode nd = nodes[id];
+  const uint32_t i = pre[id];
+  for (int k = 0; k < 2 * D; ++k) node_bounds[size_t(i) * 2 * D + k] = lbounds[size_t(id) * 2 * D + k];
+  if (nd.a == kNone) {
+    child_a[i] = nd.s;
+    child_b[i] = 0;
+    prim_count[i] = nd.e - nd.s;
+  } else {
+    child_a[i] = pre[nd.a];
+    child_b[i] = pre[nd.b];
+    prim_count[i] = 0;
+  }
+}
+
+inline uint32_t blocks_for(uint64_t n, uint32_t t) { return uint32_t(std::max<uint64_t>(1, (n + t - 1) / t)); }
+
+}  // namespace
+
+extern "C" int32_t sq_tree_build_d(sq_ctx* ctx, int32_t dim, uint32_t n, const float* d_prim_aabbs,
+                                   uint32_t node_capacity, uint32_t* n_nodes_out, float* d_node_bounds,
+                                   uint32_t* d_child_a, uint32_t* d_child_b, uint32_t* d_prim_count,
+                                   uint32_t* d_prim_indices) {
+  using sqi::fail;
+  if (!ctx || !n_nodes_out) return SQ_ERR_INVALID;
+  *n_nodes_out = 0;
+  if (dim < 1 || dim > kMaxDim) return fail(ctx, SQ_ERR_INVALID, "dim must be 1..8");
+  if (n == 0) return SQ_OK;
+  if (!d_prim_aabbs || !d_node_bounds || !d_child_a || !d_child_b || !d_prim_count || !d_prim_indices)
+    return fail(ctx, SQ_ERR_INVALID, "null tree array");
+  if (uint64_t(node_capacity) < 2ull * n - 1) return fail(ctx, SQ_ERR_CAPACITY, "node_capacity below 2n - 1");
+  if (n >= sq::kLeafBit) return fail(ctx, SQ_ERR_INVALID, "too many primitives");
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const int D = dim;
+  const size_t N2 = size_t(2) * n;  // node capacity of the level-order arrays
+
+  // Scratch, carved from one stream-ordered allocation.
+  sqi::Carve cv;
+  const size_t o_keys = cv.take(size_t(D) * n * 4), o_idx0 = cv.take(size_t(n) * 4), o_idx1 = cv.take(size_t(n) * 4),
+               o_sk0 = cv.take(size_t(n) * 4), o_sk1 = cv.take(size_t(n) * 4),
+               o_seg0 = cv.take((size_t(n) + 1) * sizeof(Seg)), o_seg1 = cv.take((size_t(n) + 1) * sizeof(Seg)),
+               o_beg = cv.take(size_t(n) * 4), o_end = cv.take(size_t(n) * 4), o_nodes = cv.take(N2 * sizeof(LNode)),
+               o_lb = cv.take(N2 * 2 * D * 4), o_size = cv.take(N2 * 4), o_pre = cv.take(N2 * 4), o_ctr = cv.take(16);
+  char* base = nullptr;
+  CK(cudaMallocAsync(reinterpret_cast<void**>(&base), cv.off, st));
+  uint32_t* keys = reinterpret_cast<uint32_t*>(base + o_keys);
+  uint32_t* idx = reinterpret_cast<uint32_t*>(base + o_idx0);
+  uint32_t* idx_alt = reinterpret_cast<uint32_t*>(base + o_idx1);
+  uint32_t* skeys = reinterpret_cast<uint32_t*>(base + o_sk0);
+  uint32_t* skeys_alt = reinterpret_cast<uint32_t*>(base + o_sk1);
+  Seg* cur = reinterpret_cast<Seg*>(base + o_seg0);
+  Seg* nxt = reinterpret_cast<Seg*>(base + o_seg1);
+  uint32_t* sbeg = reinterpret_cast<uint32_t*>(base + o_beg);
+  uint32_t* send = reinterpret_cast<uint32_t*>(base + o_end);
+  LNode* nodes = reinterpret_cast<LNode*>(base + o_nodes);
+  float* lbounds = reinterpret_cast<float*>(base + o_lb);
+  uint32_t* size = reinterpret_cast<uint32_t*>(base + o_size);
+  uint32_t* pre = reinterpret_cast<uint32_t*>(base + o_pre);
+  uint32_t* ctr = reinterpret_cast<uint32_t*>(base + o_ctr);
+  void* temp = nullptr;
+  size_t temp_cap = 0;
+  int32_t rc = SQ_OK;
+  auto done = [&](int32_t code) {
+    if (temp) cudaFreeAsync(temp, st);
+    cudaFreeAsync(base, st);
+    return code;
+  };
+#define CKB(x)                                                  \
+  do {                                                          \
+    cudaError_t e_ = (x);                                       \
+    if (e_ != cudaSuccess) return done(cuda_fail(ctx, #x, e_)); \
+  } while (0)
+
+  keys_kernel<<<std::min<uint32_t>(blocks_for(n, 256), 148 * 16), 256, 0, st>>>(d_prim_aabbs, n, D, keys, idx);
+  CKB(cudaGetLastError());
+  const Seg root{0, n, 0};
+  CKB(cudaMemcpyAsync(cur, &root, sizeof(Seg), cudaMemcpyHostToDevice, st));
+  const uint32_t init[4] = {0, 1, 0, 0};
+  CKB(cudaMemcpyAsync(ctr, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  std::vector<std::pair<uint32_t, uint32_t>> levels;  // level-order id ranges
+  uint32_t m = 1, made = 1;
+  while (m > 0) {
+    levels.emplace_back(made - m, made);
+    CKB(cudaMemsetAsync(ctr, 0, 4, st));      // next segments
+    CKB(cudaMemsetAsync(ctr + 2, 0, 4, st));  // sort segments
+    LevelParams p{d_prim_aabbs, D, n, keys, idx, cur, m, nxt, ctr, nodes, lbounds, sbeg, send, skeys};
+    if (m < 1024) level_kernel<256><<<m, 256, 0, st>>>(p);
+    else level_kernel<32><<<blocks_for(m, 8), 256, 0, st>>>(p);
+    CKB(cudaGetLastError());
+    uint32_t h[4];
+    CKB(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CKB(cudaStreamSynchronize(st));
+    const uint32_t n_next = h[0], n_sort = h[2];
+    made = h[1];
+    if (n_sort > 0) {
+      // Positions outside the sorted segments keep their primitive.
+      CKB(cudaMemcpyAsync(idx_alt, idx, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
+      size_t need = 0;
+      CKB(cub::DeviceSegmentedSort::StableSortPairs(nullptr, need, skeys, skeys_alt, idx, idx_alt, int(n), int(n_sort),
+                                                    sbeg, send, st));
+      if (need > temp_cap) {
+        if (temp) CKB(cudaFreeAsync(temp, st));
+        temp = nullptr;
+        temp_cap = 0;
+        CKB(cudaMallocAsync(&temp, need, st));
+        temp_cap = need;
+      }
+      CKB(cub::DeviceSegmentedSort::StableSortPairs(temp, need, skeys, skeys_alt, idx, idx_alt, int(n), int(n_sort),
+                                                    sbeg, send, st));
+      std::swap(idx, idx_alt);
+    }
+    std::swap(cur, nxt);
+    m = n_next;
+  }
+  const uint32_t n_nodes = made;
+  if (n_nodes > node_capacity) return done(fail(ctx, SQ_ERR_CAPACITY, "node_capacity too small"));
+  for (size_t L = levels.size(); L-- > 0;) {
+    const auto [lb, le] = levels[L];
+    sizes_kernel<<<blocks_for(le - lb, 256), 256, 0, st>>>(nodes, lb, le, size);
+  }
+  CKB(cudaMemsetAsync(pre, 0, 4, st));
+  for (const auto& [lb, le] : levels) preorder_kernel<<<blocks_for(le - lb, 256), 256, 0, st>>>(nodes, lb, le, size, pre);
+  emit_kernel<<<blocks_for(n_nodes, 256), 256, 0, st>>>(nodes, lbounds, pre, n_nodes, D, d_node_bounds, d_child_a,
+                                                        d_child_b, d_prim_count);
+  CKB(cudaGetLastError());
+  CKB(cudaMemcpyAsync(d_prim_indices, idx, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
+  ctx->launches += 2 + 2 * levels.size() + 1;
+  rc = done(SQ_OK);
+  CK(cudaStreamSynchronize(st));
+  *n_nodes_out = n_nodes;
+#undef CKB
+  return rc;
+}
