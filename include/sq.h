@@ -209,8 +209,14 @@ int32_t sq_bvh_upload(sq_ctx* ctx, int32_t dim, int32_t narrow, uint32_t n_nodes
  * past max_toi) and normal[3] for a hit. The library's exact maths
  * (fadd, fmul, ray_at, ...) are in scope. prim_aabbs (min[3], max[3] per
  * leaf) are the boxes the tree was built from; each must contain its
- * leaf's hits (near-first answers are certified against them). Ray nearest
- * and all-hits queries are supported; casts, overlaps and refit return
+ * leaf's hits (near-first answers are certified against them). The source
+ * may also define every crossing of a leaf (QueryGeometry::
+ * test_ray_crossings, query/geometry.rs), which raycast_crossings then lists:
+ *   template <class Emit>
+ *   __device__ void sq_narrow_crossings(const float* prim, uint32_t leaf,
+ *       const float* ro, const float* rd, float max_toi, Emit& emit);
+ * calling emit(toi, normal) per crossing. Ray nearest, all-hits and
+ * crossings queries are supported; casts, overlaps and refit return
  * SQ_ERR_UNSUPPORTED. A source that does not compile returns SQ_ERR_COMPILE
  * with the compiler log in sq_ctx_last_error. Kernels are cached per source
  * and stride for the process. */
@@ -249,7 +255,9 @@ int32_t sq_raycast_all_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_rays, ui
                          sq_query_stats* stats);
 
 /* raycast_crossings (accel/bvh.rs:261-328): every entry and exit of sphere
- * leaves; one crossing per hit for the other narrow phases. */
+ * leaves; every crossing a consumer narrow phase emits when its source also
+ * defines sq_narrow_crossings (see sq_bvh_upload_custom); one crossing per
+ * hit for the other narrow phases. */
 int32_t sq_raycast_crossings(sq_ctx* ctx, const sq_bvh* bvh, const float* rays, uint32_t n, float max_toi,
                              const float* max_toi_per_query, const sq_filter* filter, const sq_hit_lists* out);
 int32_t sq_raycast_crossings_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_rays, uint32_t n, float max_toi,

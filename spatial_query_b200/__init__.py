@@ -473,7 +473,8 @@ class DeviceBvh:
         prims: [n, stride] leaf parameters; aabbs: [n, 6] the boxes the tree
         was built from."""
         prims = np.ascontiguousarray(prims, dtype=np.float32)
-        prims = prims.reshape(prims.shape[0], -1)
+        if prims.ndim != 2:
+            prims = prims.reshape(prims.shape[0], -1)
         aabbs = np.ascontiguousarray(aabbs, dtype=np.float32).reshape(-1, 6)
         self = cls.__new__(cls)
         self.ctx, self.dim, self.geom, self.tree = ctx, 3, None, tree

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <nvrtc.h>
 
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
@@ -51,7 +52,11 @@ int32_t rtc_kernel_set(uint32_t stride, const char* src, sq::KernelSet* out, std
     *out = it->second.ks;
     return SQ_OK;
   }
+  // A source that defines sq_narrow_crossings also serves raycast_crossings
+  // with every crossing it emits.
+  const bool crossings = std::strstr(src, "sq_narrow_crossings") != nullptr;
   const std::string prog_src = "#define SQ_RTC_CUSTOM 1\n#define SQ_CUSTOM_STRIDE " + std::to_string(stride) +
+                               (crossings ? "\n#define SQ_RTC_CROSSINGS 1" : "") +
                                "\n#include \"traverse.cuh\"\nnamespace sq {\n#line 1 \"narrow\"\n" + src +
                                "\n}  // namespace sq\n";
   const char* headers[2] = {kRtcMath, kRtcTraverse};

@@ -40,6 +40,18 @@ enum Narrow : int { kNarrowAabb = 0, kNarrowSphere = 1, kNarrowSphereNear = 2, k
 __device__ bool sq_narrow(const float* prim, uint32_t leaf, const float* ro, const float* rd, float max_toi, float* toi,
                           float* normal);
 #endif
+// Optionally the source also defines every crossing of a leaf
+// (QueryGeometry::test_ray_crossings, consumed by Bvh::raycast_crossings,
+// accel/bvh.rs:286-328); SQ_RTC_CROSSINGS is then defined and
+// raycast_crossings lists each emit(toi, normal) call:
+//   template <class Emit>
+//   __device__ void sq_narrow_crossings(const float* prim, uint32_t leaf, const float* ro, const float* rd,
+//                                       float max_toi, Emit& emit);
+#ifdef SQ_RTC_CROSSINGS
+template <class Emit>
+__device__ void sq_narrow_crossings(const float* prim, uint32_t leaf, const float* ro, const float* rd, float max_toi,
+                                    Emit& emit);
+#endif
 enum QKind : int { kRayNearest = 0, kRayAll = 1, kCastNearest = 2, kCastAll = 3, kOverlap = 4 };
 
 constexpr int kThreads = 128;
@@ -573,9 +585,25 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
                 if (STATS) L.v_hit += 1;
                 list_insert<D>(p, L.q, L.count, t, id, nrm);
               }
-            } else if (narrow_ray<D, N>(rec, L.r, L.limit, t, nrm)) {
-              if (STATS) L.v_hit += 1;
-              list_insert<D>(p, L.q, L.count, t, id, nrm);
+            } else {
+              bool listed = false;
+#ifdef SQ_RTC_CROSSINGS
+              if constexpr (N == kNarrowCustom) {
+                if (p.crossings) {
+                  // Every crossing the consumer emits is listed, as bvh.rs:309-315 pushes them.
+                  auto emit = [&](float tt, const float* nn) {
+                    if (STATS) L.v_hit += 1;
+                    list_insert<D>(p, L.q, L.count, tt, id, nn);
+                  };
+                  sq_narrow_crossings(rec, id, L.r.o, L.r.d, L.limit, emit);
+                  listed = true;
+                }
+              }
+#endif
+              if (!listed && narrow_ray<D, N>(rec, L.r, L.limit, t, nrm)) {
+                if (STATS) L.v_hit += 1;
+                list_insert<D>(p, L.q, L.count, t, id, nrm);
+              }
             }
           } else {  // kCastAll
             if (narrow_cast<D, N>(rec, L.r, L.pmin, L.pmax, L.limit, t, nrm)) list_insert<D>(p, L.q, L.count, t, id, nrm);
