@@ -187,6 +187,32 @@ int32_t sq_tree_build_d(sq_ctx* ctx, int32_t dim, uint32_t n, const float* d_pri
 /* The world AABB of each built-in leaf (the providers' world_aabb). */
 int32_t sq_prim_aabbs(int32_t dim, int32_t narrow, uint32_t n, const float* prim_data, float* out_aabbs);
 
+/* ---- the crate's f64 feature (Scalar = f64, maths/point.rs:14-18) ---------
+ * The same tree and leaf AABBs in double precision (centroids, EPSILON and
+ * total_cmp of f64), for scenes uploaded with sq_bvh_upload_f64. */
+int32_t sq_tree_build_f64(int32_t dim, uint32_t n, const double* prim_aabbs, int32_t threads, uint32_t node_capacity,
+                          uint32_t* n_nodes_out, double* node_bounds, uint32_t* child_a, uint32_t* child_b,
+                          uint32_t* prim_count, uint32_t* prim_indices);
+int32_t sq_prim_aabbs_f64(int32_t dim, int32_t narrow, uint32_t n, const double* prim_data, double* out_aabbs);
+/* An f64 scene: the host tree (tree::Node arrays with double bounds) and
+ * double leaf parameters (built-in narrow phases, same layouts as
+ * sq_bvh_upload); layers optional. It answers only the _f64 queries; the f32
+ * entry points return SQ_ERR_UNSUPPORTED for it. */
+int32_t sq_bvh_upload_f64(sq_ctx* ctx, int32_t dim, int32_t narrow, uint32_t n_nodes, const double* node_bounds,
+                          const uint32_t* child_a, const uint32_t* child_b, const uint32_t* prim_count,
+                          uint32_t n_prims, const uint32_t* prim_indices, const double* prim_data,
+                          uint32_t prim_stride, const uint64_t* layers, sq_bvh** out);
+/* Bvh::raycast_nearest with Scalar = f64 (accel/bvh.rs:73-124), walked in the
+ * crate's own order: leaf, toi and normal (D doubles) equal the f64 CPU
+ * path's, and so do the QueryStats counters (stats may be NULL). A miss gives
+ * SQ_NO_HIT, toi 0 and a zero normal. toi / normal may be NULL. */
+int32_t sq_raycast_nearest_f64(sq_ctx* ctx, const sq_bvh* bvh, const double* rays, uint32_t n, double max_toi,
+                               const double* max_toi_per_query, const sq_filter* filter, uint32_t* leaf,
+                               double* toi, double* normal, sq_query_stats* stats);
+int32_t sq_raycast_nearest_f64_d(sq_ctx* ctx, const sq_bvh* bvh, const double* d_rays, uint32_t n, double max_toi,
+                                 const double* d_max_toi_per_query, const sq_filter* filter, uint32_t* d_leaf,
+                                 double* d_toi, double* d_normal, sq_query_stats* stats);
+
 /* ---- scene upload (GpuRaycaster::new, gpu/mod.rs:252-303) -------------------
  * Takes the host tree as tree::Node arrays (accel/tree.rs:21-26; Bvh::nodes
  * and Bvh::prim_indices, accel/bvh.rs:463-475) and the leaf parameters indexed

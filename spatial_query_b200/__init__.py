@@ -101,6 +101,12 @@ SIGNATURES = {
     "sq_tree_build": (C.c_int32, [C.c_int32, C.c_uint32, P, C.c_int32, C.c_uint32, P, P, P, P, P, P]),
     "sq_prim_aabbs": (C.c_int32, [C.c_int32, C.c_int32, C.c_uint32, P, P]),
     "sq_tree_build_d": (C.c_int32, [P, C.c_int32, C.c_uint32, P, C.c_uint32, P, P, P, P, P, P]),
+    "sq_tree_build_f64": (C.c_int32, [C.c_int32, C.c_uint32, P, C.c_int32, C.c_uint32, P, P, P, P, P, P]),
+    "sq_prim_aabbs_f64": (C.c_int32, [C.c_int32, C.c_int32, C.c_uint32, P, P]),
+    "sq_bvh_upload_f64": (C.c_int32, [P, C.c_int32, C.c_int32, C.c_uint32, P, P, P, P, C.c_uint32, P, P, C.c_uint32,
+                                      P, P]),
+    "sq_raycast_nearest_f64": (C.c_int32, [P, P, P, C.c_uint32, C.c_double, P, P, P, P, P, P]),
+    "sq_raycast_nearest_f64_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_double, P, P, P, P, P, P]),
     "sq_autotune_nearest_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, C.c_uint32, P]),
     "sq_bvh_upload_custom": (C.c_int32, [P, C.c_uint32, P, P, P, P, C.c_uint32, P, P, C.c_uint32, P, C.c_char_p,
                                          C.POINTER(P)]),
@@ -235,6 +241,16 @@ class Geometry:
             raise SqError(rc, "sq_prim_aabbs")
         return out
 
+    def world_aabbs_f64(self, prims64: Optional[np.ndarray] = None) -> np.ndarray:
+        """The leaf AABBs in f64 (sq_prim_aabbs_f64) of `prims64` (default:
+        this geometry's parameters widened to double)."""
+        p = np.ascontiguousarray(self.prims if prims64 is None else prims64, dtype=np.float64)
+        out = np.empty((self.leaf_count, 2 * self.dim), np.float64)
+        rc = lib().sq_prim_aabbs_f64(self.dim, NARROW[self.narrow], self.leaf_count, _p(p), _p(out))
+        if rc:
+            raise SqError(rc, "sq_prim_aabbs_f64")
+        return out
+
 
 @dataclass
 class HostBvh:
@@ -270,6 +286,23 @@ class HostBvh:
     @classmethod
     def build(cls, geom: Geometry, threads: int = 0) -> "HostBvh":
         return cls.build_from_aabbs(geom.dim, geom.world_aabbs(), threads)
+
+    @classmethod
+    def build_f64(cls, dim: int, aabbs: np.ndarray, threads: int = 0) -> "HostBvh":
+        """The crate's tree with Scalar = f64 (sq_tree_build_f64): double bounds."""
+        aabbs = np.ascontiguousarray(aabbs, dtype=np.float64).reshape(-1, 2 * dim)
+        n = aabbs.shape[0]
+        cap = max(2 * n - 1, 1)
+        b = np.empty((cap, 2 * dim), np.float64)
+        ca, cb, pc = (np.empty(cap, np.uint32) for _ in range(3))
+        pi = np.empty(max(n, 1), np.uint32)
+        nn = C.c_uint32(0)
+        rc = lib().sq_tree_build_f64(dim, n, _p(aabbs), threads, cap, C.byref(nn), _p(b), _p(ca), _p(cb), _p(pc),
+                                     _p(pi))
+        if rc:
+            raise SqError(rc, "sq_tree_build_f64")
+        k = nn.value
+        return cls(dim, b[:k].copy(), ca[:k].copy(), cb[:k].copy(), pc[:k].copy(), pi[:n].copy())
 
     @classmethod
     def build_on_device(cls, ctx: "Context", dim: int, aabbs: np.ndarray) -> "HostBvh":
@@ -640,6 +673,55 @@ class GpuHit:
     point: np.ndarray
     normal: np.ndarray
     sub_object: Optional[int] = None
+
+
+class DeviceBvh64:
+    """An f64 scene (sq_bvh_upload_f64): the crate's `f64` feature on the
+    device. `tree` is a HostBvh with double bounds (HostBvh.build_f64);
+    `prims64` the leaf parameters in double."""
+
+    def __init__(self, ctx: Context, tree: HostBvh, geom: Geometry, prims64: Optional[np.ndarray] = None):
+        self.ctx, self.dim, self.geom = ctx, geom.dim, geom
+        self.prims64 = np.ascontiguousarray(geom.prims if prims64 is None else prims64, dtype=np.float64)
+        self._layers = None if geom.layers is None else np.ascontiguousarray(geom.layers, dtype=np.uint64)
+        bounds = np.ascontiguousarray(tree.bounds, dtype=np.float64)
+        h = P()
+        nn = tree.node_count
+        z = np.zeros(4, np.uint32)
+        zd = np.zeros(4, np.float64)
+        ctx.check(lib().sq_bvh_upload_f64(ctx.h, geom.dim, NARROW[geom.narrow], nn, _p(bounds if nn else zd),
+                                          _p(tree.child_a if nn else z), _p(tree.child_b if nn else z),
+                                          _p(tree.prim_count if nn else z), geom.leaf_count,
+                                          _p(tree.prim_indices if nn else z),
+                                          _p(self.prims64 if geom.leaf_count else zd), geom.stride,
+                                          _p(self._layers), C.byref(h)), "sq_bvh_upload_f64")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.sq_bvh_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def raycast_nearest(self, rays, max_toi, mask=None, exclude=None, stats=False) -> Hits:
+        """rays: [n, 2D] doubles; max_toi a scalar or one per ray."""
+        rays = np.ascontiguousarray(rays, dtype=np.float64).reshape(-1, 2 * self.dim)
+        n = rays.shape[0]
+        per = np.ndim(max_toi) > 0
+        mt = np.ascontiguousarray(max_toi, dtype=np.float64) if per else None
+        leaf = np.empty(n, np.uint32)
+        toi = np.empty(n, np.float64)
+        nrm = np.empty((n, self.dim), np.float64)
+        st = _Stats() if stats else None
+        self.ctx.check(lib().sq_raycast_nearest_f64(self.ctx.h, self.h, _p(rays), n, 0.0 if per else float(max_toi),
+                                                    _p(mt), _filter(mask, exclude), _p(leaf), _p(toi), _p(nrm),
+                                                    C.byref(st) if st is not None else None),
+                       "sq_raycast_nearest_f64")
+        sd = None if st is None else dict(nodes_visited=st.nodes_visited, aabb_tests=st.aabb_tests,
+                                          narrow_tests=st.narrow_tests, hits=st.hits)
+        return Hits(leaf, toi, nrm, None, None, sd)
 
 
 class GpuRaycaster:

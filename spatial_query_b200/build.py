@@ -31,6 +31,7 @@ UNITS = [
     ("tlas_kernels.cu", ["--fmad=false"]),
     ("guide.cu", []),
     ("tree_build_gpu.cu", ["--fmad=false"]),
+    ("sq_f64.cu", ["--fmad=false"]),
     ("rtc.cu", ["-I", BUILD]),
     ("tree_build.cpp", []),
 ]

@@ -943,7 +943,7 @@ extern "C" int32_t sq_guide_destroy(sq_guide* g) {
 extern "C" int32_t sq_guide_create(sq_ctx* ctx, const sq_bvh* b, const sq_guide_config* cfg, sq_guide** out) {
   if (!ctx || !b || !out) return SQ_ERR_INVALID;
   *out = nullptr;
-  if (b->dim != 3) return fail(ctx, SQ_ERR_UNSUPPORTED, "the learned guide needs a D = 3 scene");
+  if (b->dim != 3 || b->prec != 32) return fail(ctx, SQ_ERR_UNSUPPORTED, "the learned guide needs a D = 3 f32 scene");
   if (b->n_nodes == 0) return fail(ctx, SQ_ERR_INVALID, "the learned guide needs a non-empty scene");
   sq_guide_config c;
   sq_guide_config_default(&c);

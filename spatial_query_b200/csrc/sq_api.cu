@@ -46,6 +46,7 @@ int32_t check_scene(sq_ctx* ctx, const sq_bvh* b) {
   if (!ctx) return SQ_ERR_INVALID;
   if (!b) return fail(ctx, SQ_ERR_INVALID, "null scene");
   if (b->device != ctx->device) return fail(ctx, SQ_ERR_INVALID, "scene and context are on different devices");
+  if (b->prec != 32) return fail(ctx, SQ_ERR_UNSUPPORTED, "an f64 scene is queried through the _f64 entry points");
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_fail(ctx, "cudaSetDevice", e);
   return SQ_OK;
@@ -441,7 +442,8 @@ extern "C" int32_t sq_bvh_destroy(sq_bvh* b) {
   if (!b) return SQ_OK;
   cudaSetDevice(b->device);
   void* ptrs[] = {b->d_nodes, b->d_prims, b->d_root, b->d_layers, b->d_sub, b->d_prim_ids,
-                  b->d_leaves, b->d_parents, b->d_arrivals, b->d_refit_in, b->d_nonfinite};
+                  b->d_leaves, b->d_parents, b->d_arrivals, b->d_refit_in, b->d_nonfinite,
+                  b->d_nb64, b->d_nc64, b->d_prims64};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete b;

@@ -77,6 +77,12 @@ struct sq_bvh {
   size_t bytes = 0;
   std::vector<uint32_t> h_iidx;  // host node -> interior record (or kNoHit)
   std::vector<uint32_t> h_child_a, h_child_b, h_count;
+  // An f64 scene (sq_bvh_upload_f64): node boxes, node links and leaf
+  // parameters in double, answered only by the _f64 entry points.
+  int prec = 32;
+  double* d_nb64 = nullptr;   // [n_nodes][2D]
+  uint2* d_nc64 = nullptr;    // [n_nodes]: (child_a, child_b), or (first, count | kLeafBit)
+  double* d_prims64 = nullptr;  // [n_prims][stride], leaf order
 };
 
 namespace sqi {

@@ -1,11 +1,12 @@
 // Exact device maths for the batched-query kernels.
 //
 // Every function restates the spatial-query CPU expression it replaces, in the
-// same order of IEEE f32 operations, so a hit's toi and identity are
-// bit-identical to the reference CPU path. All arithmetic goes through the
-// _rn intrinsics, which the compiler never contracts into an FMA (the files are
-// additionally compiled with --fmad=false), and division / sqrt are the
-// correctly rounded IEEE forms.
+// same order of IEEE operations, so a hit's toi and identity are bit-identical
+// to the reference CPU path. All arithmetic goes through the _rn intrinsics,
+// which the compiler never contracts into an FMA (the files are additionally
+// compiled with --fmad=false), and division / sqrt are the correctly rounded
+// IEEE forms. The scalar type S is float (the crate's default) or double (its
+// `f64` feature, maths/point.rs:14-18); float is the default everywhere.
 #pragma once
 
 #ifdef __CUDACC_RTC__
@@ -24,43 +25,69 @@ constexpr float kEps = 1.1920928955078125e-7f;  // f32::EPSILON
 constexpr uint32_t kNoHit = 0xFFFFFFFFu;
 constexpr uint32_t kLeafBit = 0x80000000u;
 
+// Per-scalar constants: EPSILON (f32 / f64) and the triangle test's two
+// literals (viewport-lib-query/src/lib.rs:295-320), in the scalar's precision.
+template <class S> struct Lim;
+template <> struct Lim<float> {
+  static constexpr float eps = 1.1920928955078125e-7f;  // f32::EPSILON
+  static constexpr float tri_det = 1e-8f;
+  static constexpr float tri_t = 1e-6f;
+};
+template <> struct Lim<double> {
+  static constexpr double eps = 2.220446049250313080847e-16;  // f64::EPSILON
+  static constexpr double tri_det = 1e-8;
+  static constexpr double tri_t = 1e-6;
+};
+
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
 __device__ __forceinline__ float fsqrt(float a) { return __fsqrt_rn(a); }
+__device__ __forceinline__ float sabs(float a) { return fabsf(a); }
+__device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double fsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double fdiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double fsqrt(double a) { return __dsqrt_rn(a); }
+__device__ __forceinline__ double sabs(double a) { return fabs(a); }
 
-// Rust's f32::total_cmp as a signed key.
+// Rust's f32::total_cmp / f64::total_cmp as signed keys.
 __device__ __forceinline__ int32_t total_key(float x) {
   int32_t b = __float_as_int(x);
   return b ^ int32_t(uint32_t(b >> 31) >> 1);
 }
+__device__ __forceinline__ int64_t total_key(double x) {
+  int64_t b = __double_as_longlong(x);
+  return b ^ int64_t(uint64_t(b >> 63) >> 1);
+}
 
 // hit_ordering (query/hit.rs:77-84): is (ta, la) strictly before (tb, lb)?
-__device__ __forceinline__ bool hit_before(float ta, uint32_t la, float tb, uint32_t lb) {
-  int32_t ka = total_key(ta), kb = total_key(tb);
+template <class S>
+__device__ __forceinline__ bool hit_before(S ta, uint32_t la, S tb, uint32_t lb) {
+  const auto ka = total_key(ta), kb = total_key(tb);
   return ka < kb || (ka == kb && la < lb);
 }
 
 // A ray or sweep with its per-axis reciprocals: inv[i] = 1 / d[i] is the value
 // Aabb::ray_intersect recomputes at every node (aabb.rs:130); bit i of `par`
 // marks an axis with |d| < EPSILON (the parallel-slab branch, aabb.rs:124-128).
-template <int D> struct RayPre {
-  float o[D];
-  float d[D];
-  float inv[D];
+template <int D, class S = float> struct RayPre {
+  S o[D];
+  S d[D];
+  S inv[D];
   uint32_t par;
 };
 
-template <int D> __device__ __forceinline__ void ray_prep(RayPre<D>& r) {
+template <int D, class S> __device__ __forceinline__ void ray_prep(RayPre<D, S>& r) {
   r.par = 0;
 #pragma unroll
   for (int i = 0; i < D; ++i) {
-    if (fabsf(r.d[i]) < kEps) {
+    if (sabs(r.d[i]) < Lim<S>::eps) {
       r.par |= 1u << i;
-      r.inv[i] = 0.f;
+      r.inv[i] = S(0);
     } else {
-      r.inv[i] = fdiv(1.0f, r.d[i]);
+      r.inv[i] = fdiv(S(1), r.d[i]);
     }
   }
 }
@@ -69,10 +96,10 @@ template <int D> __device__ __forceinline__ void ray_prep(RayPre<D>& r) {
 // t_min > t_max; t_min only grows and t_max only shrinks along the axes, so
 // testing once at the end gives the same outcome. Returns pass and the entry
 // parameter; `axis` is the last axis that raised t_min (-1: none).
-template <int D>
-__device__ __forceinline__ bool slab(const RayPre<D>& r, const float* lo, const float* hi, float max_toi,
-                                     float& t_enter, int& axis) {
-  float tmin = 0.f, tmax = max_toi;
+template <int D, class S>
+__device__ __forceinline__ bool slab(const RayPre<D, S>& r, const S* lo, const S* hi, S max_toi, S& t_enter,
+                                     int& axis) {
+  S tmin = S(0), tmax = max_toi;
   bool ok = true;
   axis = -1;
 #pragma unroll
@@ -80,9 +107,9 @@ __device__ __forceinline__ bool slab(const RayPre<D>& r, const float* lo, const 
     if (r.par & (1u << i)) {
       ok = ok && !(r.o[i] < lo[i] || r.o[i] > hi[i]);
     } else {
-      float t1 = fmul(fsub(lo[i], r.o[i]), r.inv[i]);
-      float t2 = fmul(fsub(hi[i], r.o[i]), r.inv[i]);
-      if (t1 > t2) { float t = t1; t1 = t2; t2 = t; }
+      S t1 = fmul(fsub(lo[i], r.o[i]), r.inv[i]);
+      S t2 = fmul(fsub(hi[i], r.o[i]), r.inv[i]);
+      if (t1 > t2) { S t = t1; t1 = t2; t2 = t; }
       if (t1 > tmin) { tmin = t1; axis = i; }
       if (t2 < tmax) tmax = t2;
     }
@@ -141,8 +168,8 @@ __device__ __forceinline__ bool slab_grown_fast(const RayPre<D>& r, const float*
 }
 
 // Aabb::intersects (aabb.rs:101-108): touching faces count.
-template <int D> __device__ __forceinline__ bool box_overlap(const float* lo, const float* hi, const float* qlo,
-                                                             const float* qhi) {
+template <int D, class S> __device__ __forceinline__ bool box_overlap(const S* lo, const S* hi, const S* qlo,
+                                                                      const S* qhi) {
   bool ok = true;
 #pragma unroll
   for (int i = 0; i < D; ++i) ok = ok && !(lo[i] > qhi[i] || hi[i] < qlo[i]);
@@ -150,58 +177,57 @@ template <int D> __device__ __forceinline__ bool box_overlap(const float* lo, co
 }
 
 // Point::dot (point.rs:60-66): accumulate from 0.0 in index order.
-template <int D> __device__ __forceinline__ float pdot(const float* a, const float* b) {
-  float acc = 0.f;
+template <int D, class S> __device__ __forceinline__ S pdot(const S* a, const S* b) {
+  S acc = S(0);
 #pragma unroll
   for (int i = 0; i < D; ++i) acc = fadd(acc, fmul(a[i], b[i]));
   return acc;
 }
 
 // Point::normalize_or_zero (point.rs:82-89), in place.
-template <int D> __device__ __forceinline__ void normalize_or_zero(float* v) {
-  float len = fsqrt(pdot<D>(v, v));
-  if (len > kEps) {
-    float s = fdiv(1.0f, len);
+template <int D, class S> __device__ __forceinline__ void normalize_or_zero(S* v) {
+  S len = fsqrt(pdot<D>(v, v));
+  if (len > Lim<S>::eps) {
+    S s = fdiv(S(1), len);
 #pragma unroll
     for (int i = 0; i < D; ++i) v[i] = fmul(v[i], s);
   } else {
 #pragma unroll
-    for (int i = 0; i < D; ++i) v[i] = 0.f;
+    for (int i = 0; i < D; ++i) v[i] = S(0);
   }
 }
 
 // Ray::at (ray.rs:33-35): origin + dir * t.
-template <int D> __device__ __forceinline__ void ray_at(const float* o, const float* d, float t, float* out) {
+template <int D, class S> __device__ __forceinline__ void ray_at(const S* o, const S* d, S t, S* out) {
 #pragma unroll
   for (int i = 0; i < D; ++i) out[i] = fadd(o[i], fmul(d[i], t));
 }
 
 // Entry-face normal: -sign(d[axis]) on `axis`, zero when axis < 0.
-template <int D> __device__ __forceinline__ void entry_normal(const float* d, int axis, float* n) {
+template <int D, class S> __device__ __forceinline__ void entry_normal(const S* d, int axis, S* n) {
 #pragma unroll
-  for (int i = 0; i < D; ++i) n[i] = (i == axis) ? ((d[i] > 0.f) ? -1.f : 1.f) : 0.f;
+  for (int i = 0; i < D; ++i) n[i] = (i == axis) ? ((d[i] > S(0)) ? S(-1) : S(1)) : S(0);
 }
 
 // Ray against a ball (tests/differential.rs:61-82; near-root-only variant
 // tests/gpu.rs:92-106): the near root, or the far root when the origin is
 // inside (FAR). Writes toi and the outward normal.
-template <int D, bool FAR>
-__device__ __forceinline__ bool ray_ball(const float* o, const float* d, const float* c, float r, float max_toi,
-                                         float& t_out, float* n_out) {
-  float oc[D];
+template <int D, bool FAR, class S>
+__device__ __forceinline__ bool ray_ball(const S* o, const S* d, const S* c, S r, S max_toi, S& t_out, S* n_out) {
+  S oc[D];
 #pragma unroll
   for (int i = 0; i < D; ++i) oc[i] = fsub(o[i], c[i]);
-  float b = pdot<D>(oc, d);
-  float cc = fsub(pdot<D>(oc, oc), fmul(r, r));
-  float disc = fsub(fmul(b, b), cc);
-  if (disc < 0.f) return false;
-  float sq = fsqrt(disc);
-  float nb = -b;
-  float t = fsub(nb, sq);
-  if (FAR && t < 0.f) t = fadd(nb, sq);
-  if (t < 0.f || t > max_toi) return false;
+  S b = pdot<D>(oc, d);
+  S cc = fsub(pdot<D>(oc, oc), fmul(r, r));
+  S disc = fsub(fmul(b, b), cc);
+  if (disc < S(0)) return false;
+  S sq = fsqrt(disc);
+  S nb = -b;
+  S t = fsub(nb, sq);
+  if (FAR && t < S(0)) t = fadd(nb, sq);
+  if (t < S(0) || t > max_toi) return false;
   t_out = t;
-  float p[D];
+  S p[D];
   ray_at<D>(o, d, t, p);
 #pragma unroll
   for (int i = 0; i < D; ++i) n_out[i] = fsub(p[i], c[i]);
@@ -211,10 +237,10 @@ __device__ __forceinline__ bool ray_ball(const float* o, const float* d, const f
 
 // glam Vec3 dot / cross, the operations of the reference triangle test
 // (crates/viewport-lib-query/src/lib.rs:295-320).
-__device__ __forceinline__ float gdot(const float* a, const float* b) {
+template <class S> __device__ __forceinline__ S gdot(const S* a, const S* b) {
   return fadd(fadd(fmul(a[0], b[0]), fmul(a[1], b[1])), fmul(a[2], b[2]));
 }
-__device__ __forceinline__ void gcross(const float* a, const float* b, float* o) {
+template <class S> __device__ __forceinline__ void gcross(const S* a, const S* b, S* o) {
   o[0] = fsub(fmul(a[1], b[2]), fmul(b[1], a[2]));
   o[1] = fsub(fmul(a[2], b[0]), fmul(b[2], a[0]));
   o[2] = fsub(fmul(a[0], b[1]), fmul(b[0], a[1]));
@@ -222,31 +248,31 @@ __device__ __forceinline__ void gcross(const float* a, const float* b, float* o)
 
 // Moeller-Trumbore, double-sided: |det| < 1e-8 rejects, u in [0, 1], v >= 0,
 // u + v <= 1, t > 1e-6; the caller bounds t by max_toi.
-__device__ __forceinline__ bool ray_triangle(const float* o, const float* d, const float* v0, const float* v1,
-                                             const float* v2, float& t_out) {
-  float e1[3], e2[3], p[3], tv[3], q[3];
+template <class S>
+__device__ __forceinline__ bool ray_triangle(const S* o, const S* d, const S* v0, const S* v1, const S* v2, S& t_out) {
+  S e1[3], e2[3], p[3], tv[3], q[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) { e1[i] = fsub(v1[i], v0[i]); e2[i] = fsub(v2[i], v0[i]); }
   gcross(d, e2, p);
-  float det = gdot(e1, p);
-  if (fabsf(det) < 1e-8f) return false;
-  float inv = fdiv(1.0f, det);
+  S det = gdot(e1, p);
+  if (sabs(det) < Lim<S>::tri_det) return false;
+  S inv = fdiv(S(1), det);
 #pragma unroll
   for (int i = 0; i < 3; ++i) tv[i] = fsub(o[i], v0[i]);
-  float u = fmul(gdot(tv, p), inv);
-  if (!(0.f <= u && u <= 1.f)) return false;
+  S u = fmul(gdot(tv, p), inv);
+  if (!(S(0) <= u && u <= S(1))) return false;
   gcross(tv, e1, q);
-  float v = fmul(gdot(d, q), inv);
-  if (v < 0.f || fadd(u, v) > 1.f) return false;
-  float t = fmul(gdot(e2, q), inv);
-  if (!(t > 1e-6f)) return false;
+  S v = fmul(gdot(d, q), inv);
+  if (v < S(0) || fadd(u, v) > S(1)) return false;
+  S t = fmul(gdot(e2, q), inv);
+  if (!(t > Lim<S>::tri_t)) return false;
   t_out = t;
   return true;
 }
 
 // Face normal: normalize_or_zero(cross(v1 - v0, v2 - v0)).
-__device__ __forceinline__ void tri_normal(const float* v0, const float* v1, const float* v2, float* n) {
-  float e1[3], e2[3];
+template <class S> __device__ __forceinline__ void tri_normal(const S* v0, const S* v1, const S* v2, S* n) {
+  S e1[3], e2[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) { e1[i] = fsub(v1[i], v0[i]); e2[i] = fsub(v2[i], v0[i]); }
   gcross(e1, e2, n);
