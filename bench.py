@@ -657,13 +657,19 @@ def main():
                        "identical_hits": identical,
                        "plain_gpu": {"value": round(plain_value, 3), "unit": "Mrays/s", "ms_per_step": round(plain_ms, 4),
                                      "path": "plain GPU traversal, autotuned: "
-                                             + ("near-first" if tune["best"]["order"] == 0 else "reference order")
+                                             + (("near-first, " + ("four-wide" if tune["best"]["layout"] == 1
+                                                                   else "child-pair") + " records")
+                                                if tune["best"]["order"] == 0 else "reference order")
                                              + f", {tune['best']['blocks_per_sm'] or 'occupancy'} blocks per SM",
                                      "e2e_mrays": round(world * n / (e2e_plain_ms / 1000) / 1e6, 3),
                                      "replayed_in_reference_order": int(replayed)},
                        "learned_vs_plain": round(value / plain_value, 4),
                        "autotune": {"best": tune["best"], "candidates": len(tune["table"]),
-                                    "near_first_best_ms": round(min(e["ms"] for e in tune["table"] if e["order"] == 0), 4),
+                                    "near_first_best_ms": round(min(e["ms"] for e in tune["table"]
+                                                                    if e["order"] == 0 and e["layout"] == 0), 4),
+                                    "four_wide_best_ms": round(min((e["ms"] for e in tune["table"]
+                                                                    if e["order"] == 0 and e["layout"] == 1),
+                                                                   default=float("nan")), 4),
                                     "reference_best_ms": round(min(e["ms"] for e in tune["table"] if e["order"] == 1), 4)},
                        "all_hits_k16": {"value": round(world * n / (all_ms / 1000) / 1e6, 3), "unit": "Mrays/s",
                                         "ms_per_step": round(all_ms, 4),

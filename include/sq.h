@@ -63,6 +63,13 @@ extern "C" {
 #define SQ_ORDER_REFERENCE 1    /* the crate's own order (accel/bvh.rs:119-120), replaying the CPU's
                                    decisions step for step (QueryStats counters included) */
 
+/* Node records walked by near-first nearest rays (sq_ctx_set_layout); both
+ * give the reference's answers. */
+#define SQ_LAYOUT_BINARY 0      /* the default: child-pair records, both children of a node in one record */
+#define SQ_LAYOUT_WIDE 1        /* four-wide records (the binary tree with every other level folded into
+                                   its parent): half the dependent fetches per ray, twice the boxes per
+                                   fetch; the autotuner picks it where it is faster */
+
 typedef struct sq_ctx sq_ctx;
 typedef struct sq_bvh sq_bvh;
 
@@ -131,6 +138,7 @@ int32_t sq_ctx_synchronize(sq_ctx* ctx);
 /* Nearest-query order (SQ_ORDER_*, default SQ_ORDER_NEAR_FIRST) and
  * persistent-grid blocks per SM (0 = occupancy). */
 int32_t sq_ctx_set_order(sq_ctx* ctx, int32_t order);
+int32_t sq_ctx_set_layout(sq_ctx* ctx, int32_t layout);
 int32_t sq_ctx_set_blocks_per_sm(sq_ctx* ctx, int32_t blocks);
 /* Near-first nearest queries prune a node only when its slab entry lies more
  * than `window` (relative, default 2^-16) past the current limit, and are
@@ -149,6 +157,7 @@ typedef struct sq_tune_entry {
   int32_t order;
   int32_t blocks_per_sm;
   float ms;
+  int32_t layout;  /* SQ_LAYOUT_* (near-first entries) */
 } sq_tune_entry;
 typedef struct sq_tune_result {
   uint32_t n_entries;

@@ -36,6 +36,8 @@ SQ_ERR_DEPTH = 5
 SQ_ERR_CAPACITY = 6
 SQ_ERR_COMPILE = 7
 NO_HIT = 0xFFFFFFFF
+LAYOUT_BINARY = 0
+LAYOUT_WIDE = 1
 NO_SUB = 0xFFFFFFFF
 
 NARROW = {"boxes": 0, "aabb": 0, "balls": 1, "sphere": 1, "balls_near": 2, "sphere_near": 2, "tris": 3,
@@ -94,6 +96,7 @@ SIGNATURES = {
     "sq_ctx_set_stream": (C.c_int32, [P, P]),
     "sq_ctx_synchronize": (C.c_int32, [P]),
     "sq_ctx_set_order": (C.c_int32, [P, C.c_int32]),
+    "sq_ctx_set_layout": (C.c_int32, [P, C.c_int32]),
     "sq_ctx_set_blocks_per_sm": (C.c_int32, [P, C.c_int32]),
     "sq_ctx_launch_count": (C.c_uint64, [P]),
     "sq_ctx_last_replay_count": (C.c_int32, [P, C.POINTER(C.c_uint32)]),
@@ -370,6 +373,10 @@ class Context:
     def set_order(self, order: int):
         self.check(lib().sq_ctx_set_order(self.h, order), "set_order")
 
+    def set_layout(self, layout: int):
+        """LAYOUT_BINARY (default) or LAYOUT_WIDE node records for near-first rays."""
+        self.check(lib().sq_ctx_set_layout(self.h, layout), "set_layout")
+
     def set_replay_window(self, window: float):
         self.check(lib().sq_ctx_set_replay_window(self.h, window), "set_replay_window")
 
@@ -460,7 +467,7 @@ def _stats_dict(s: _Stats) -> dict:
 
 
 class _TuneEntry(C.Structure):
-    _fields_ = [("order", C.c_int32), ("blocks_per_sm", C.c_int32), ("ms", C.c_float)]
+    _fields_ = [("order", C.c_int32), ("blocks_per_sm", C.c_int32), ("ms", C.c_float), ("layout", C.c_int32)]
 
 
 class _TuneResult(C.Structure):
@@ -495,8 +502,8 @@ class DeviceBvh:
         r = _TuneResult()
         self.ctx.check(lib().sq_autotune_nearest_d(self.ctx.h, self.h, _p(d_rays), n, float(max_toi), reps,
                                                    C.byref(r)), "autotune")
-        table = [dict(order=r.entries[i].order, blocks_per_sm=r.entries[i].blocks_per_sm, ms=r.entries[i].ms)
-                 for i in range(r.n_entries)]
+        table = [dict(order=r.entries[i].order, blocks_per_sm=r.entries[i].blocks_per_sm, ms=r.entries[i].ms,
+                      layout=r.entries[i].layout) for i in range(r.n_entries)]
         return dict(best=table[r.best], table=table)
 
     @classmethod

@@ -38,6 +38,8 @@ void base_params(const sq_bvh* b, const sq_filter* f, QueryParams& p) {
   p.root_box = b->d_root;
   p.nonfinite = b->d_nonfinite;
   p.root_code = b->root_code;
+  p.wnodes = b->d_wnodes;
+  p.wroot = b->wroot;
   p.mask = f ? f->layer_mask : ~0ull;
   p.exclude = f ? f->exclude : -1;
 }
@@ -85,6 +87,10 @@ int32_t nearest_core(sq_ctx* ctx, const sq_bvh* b, bool cast, const float* d_q, 
   const void* near_fn = cast ? b->ks.cast_nearest[0] : b->ks.ray_nearest[0][st];
   if (!ref_fn || !near_fn) return fail(ctx, SQ_ERR_UNSUPPORTED, "this scene's narrow phase has no such query");
   if (!near_first) return launch_persistent(ctx, ref_fn, p, b->depth, p.n);
+  // Four-wide records for plain near-first rays: each visited record stacks
+  // at most three children, so the stack holds 3 x (four-wide depth) + 1.
+  if (!cast && !stats && ctx->layout == SQ_LAYOUT_WIDE && b->n_wide && b->ks.ray_nearest_wide)
+    return near_first_launch(ctx, b, b->ks.ray_nearest_wide, ref_fn, p, 3 * b->wdepth + 1);
   return near_first_launch(ctx, b, near_fn, ref_fn, p, b->depth);
 }
 
@@ -218,6 +224,12 @@ extern "C" int32_t sq_ctx_synchronize(sq_ctx* ctx) {
 extern "C" int32_t sq_ctx_set_order(sq_ctx* ctx, int32_t order) {
   if (!ctx || (order != SQ_ORDER_NEAR_FIRST && order != SQ_ORDER_REFERENCE)) return SQ_ERR_INVALID;
   ctx->order = order;
+  return SQ_OK;
+}
+
+extern "C" int32_t sq_ctx_set_layout(sq_ctx* ctx, int32_t layout) {
+  if (!ctx || (layout != SQ_LAYOUT_BINARY && layout != SQ_LAYOUT_WIDE)) return SQ_ERR_INVALID;
+  ctx->layout = layout;
   return SQ_OK;
 }
 
@@ -380,6 +392,64 @@ static int32_t upload_impl(sq_ctx* ctx, int32_t dim, int32_t narrow, uint32_t n_
     }
   }
 
+  // Four-wide records: each binary interior node whose parent is not folded
+  // into it heads a record holding its children, with each interior child
+  // replaced by that child's two children (two to four slots). Numbered in
+  // depth-first order; slot sources point at the binary record slot that
+  // holds the same box (refit copies them from there).
+  std::vector<float> wnodes;
+  std::vector<uint32_t> wsrc;
+  if (ni > 0 && ks.ray_nearest_wide) {
+    const uint32_t WV = wide_vec(D);
+    std::vector<uint32_t> parent_slot(n_nodes, kNoHit);  // binary record << 1 | slot holding node i's box
+    for (uint32_t i = 0; i < n_nodes; ++i) {
+      if (prim_count[i] != 0) continue;
+      parent_slot[child_a[i]] = b->h_iidx[i] << 1;
+      parent_slot[child_b[i]] = (b->h_iidx[i] << 1) | 1u;
+    }
+    struct Item { uint32_t node, rec, depth; };
+    std::vector<Item> todo{{0u, 0u, 1u}};
+    wnodes.assign(size_t(WV) * 4, 0.f);
+    wsrc.assign(4, kNoHit);
+    uint32_t wdepth = 0;
+    while (!todo.empty()) {
+      const Item it = todo.back();
+      todo.pop_back();
+      wdepth = std::max(wdepth, it.depth);
+      uint32_t kids[4], nk = 0;
+      for (uint32_t c : {child_a[it.node], child_b[it.node]}) {
+        if (prim_count[c] == 0) {
+          kids[nk++] = child_a[c];
+          kids[nk++] = child_b[c];
+        } else {
+          kids[nk++] = c;
+        }
+      }
+      float* r = wnodes.data() + size_t(it.rec) * WV * 4;
+      for (uint32_t k = 0; k < 4; ++k) {
+        uint32_t code = kNoHit;
+        if (k < nk) {
+          const uint32_t c = kids[k];
+          std::memcpy(r + k * 2 * D, node_bounds + size_t(c) * 2 * D, 2 * D * 4);
+          wsrc[size_t(it.rec) * 4 + k] = parent_slot[c];
+          if (prim_count[c] != 0) {
+            code = kLeafBit | child_a[c];
+          } else {
+            code = uint32_t(wnodes.size() / (size_t(WV) * 4));
+            wnodes.resize(wnodes.size() + size_t(WV) * 4, 0.f);
+            wsrc.resize(wsrc.size() + 4, kNoHit);
+            r = wnodes.data() + size_t(it.rec) * WV * 4;  // the vector may have moved
+            todo.push_back({c, code, it.depth + 1});
+          }
+        }
+        std::memcpy(&r[8 * D + k], &code, 4);
+      }
+    }
+    b->n_wide = uint32_t(wnodes.size() / (size_t(WV) * 4));
+    b->wroot = 0;
+    b->wdepth = wdepth;
+  }
+
   auto up = [&](void** dst, const void* src, size_t bytes) -> int32_t {
     CK(cudaMalloc(dst, std::max<size_t>(bytes, 16)));
     if (src && bytes) CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
@@ -392,6 +462,10 @@ static int32_t upload_impl(sq_ctx* ctx, int32_t dim, int32_t narrow, uint32_t n_
     return code_;
   };
   if ((rc = up((void**)&b->d_nodes, nodes.data(), nodes.size() * 4))) return cleanup(rc);
+  if (b->n_wide) {
+    if ((rc = up((void**)&b->d_wnodes, wnodes.data(), wnodes.size() * 4))) return cleanup(rc);
+    if ((rc = up((void**)&b->d_wsrc, wsrc.data(), wsrc.size() * 4))) return cleanup(rc);
+  }
   if ((rc = up((void**)&b->d_prims, prims.data(), prims.size() * 4))) return cleanup(rc);
   if ((rc = up((void**)&b->d_root, node_bounds, size_t(2) * D * 4))) return cleanup(rc);
   if ((rc = up((void**)&b->d_prim_ids, prim_indices, size_t(n_prims) * 4))) return cleanup(rc);
@@ -443,7 +517,7 @@ extern "C" int32_t sq_bvh_destroy(sq_bvh* b) {
   cudaSetDevice(b->device);
   void* ptrs[] = {b->d_nodes, b->d_prims, b->d_root, b->d_layers, b->d_sub, b->d_prim_ids,
                   b->d_leaves, b->d_parents, b->d_arrivals, b->d_refit_in, b->d_nonfinite,
-                  b->d_nb64, b->d_nc64, b->d_prims64};
+                  b->d_nb64, b->d_nc64, b->d_prims64, b->d_wnodes, b->d_wsrc};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete b;
@@ -487,6 +561,16 @@ extern "C" int32_t sq_bvh_refit_d(sq_ctx* ctx, sq_bvh* b, const float* d_prim_da
   void* args[] = {&p};
   CK(cudaLaunchKernel(b->ks.refit_leaves, dim3((b->n_leaves + 255) / 256), dim3(256), args, 0, ctx->stream));
   ctx->launches++;
+  if (b->n_wide && b->ks.wide_sync) {
+    // The four-wide records take their boxes from the refit binary records.
+    float4* wn = b->d_wnodes;
+    const float4* bn = b->d_nodes;
+    const uint32_t* src = b->d_wsrc;
+    uint32_t slots = b->n_wide * 4;
+    void* wargs[] = {&wn, &bn, &src, &slots};
+    CK(cudaLaunchKernel(b->ks.wide_sync, dim3((slots + 255) / 256), dim3(256), wargs, 0, ctx->stream));
+    ctx->launches++;
+  }
   return finish(ctx);
 }
 
@@ -1057,16 +1141,21 @@ extern "C" int32_t sq_autotune_nearest_d(sq_ctx* ctx, const sq_bvh* b, const flo
   sq_hits o{};
   o.leaf = d_leaf;
   o.toi = d_toi;
-  const int saved_order = ctx->order, saved_bps = ctx->blocks_per_sm;
-  const int orders[2] = {SQ_ORDER_NEAR_FIRST, SQ_ORDER_REFERENCE};
+  const int saved_order = ctx->order, saved_bps = ctx->blocks_per_sm, saved_layout = ctx->layout;
+  // (order, layout): near-first over child-pair records, near-first over
+  // four-wide records (when the scene has them), the reference order.
+  const int orders[3] = {SQ_ORDER_NEAR_FIRST, SQ_ORDER_NEAR_FIRST, SQ_ORDER_REFERENCE};
+  const int layouts[3] = {SQ_LAYOUT_BINARY, SQ_LAYOUT_WIDE, SQ_LAYOUT_BINARY};
   const int bps[8] = {0, 2, 4, 6, 8, 10, 12, 16};
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   float best = 0.f;
-  for (int oi = 0; oi < 2 && rc == SQ_OK; ++oi) {
+  for (int oi = 0; oi < 3 && rc == SQ_OK; ++oi) {
+    if (layouts[oi] == SQ_LAYOUT_WIDE && !(b->n_wide && b->ks.ray_nearest_wide)) continue;
     for (int bi = 0; bi < 8 && rc == SQ_OK; ++bi) {
       ctx->order = orders[oi];
+      ctx->layout = layouts[oi];
       ctx->blocks_per_sm = bps[bi];
       // warm, then the best of `reps`
       if ((rc = nearest_core(ctx, b, false, d_rays, n, max_toi, nullptr, nullptr, o, false))) break;
@@ -1085,6 +1174,7 @@ extern "C" int32_t sq_autotune_nearest_d(sq_ctx* ctx, const sq_bvh* b, const flo
       e.order = orders[oi];
       e.blocks_per_sm = bps[bi];
       e.ms = t_best;
+      e.layout = layouts[oi];
       if (out->n_entries == 0 || t_best < best) {
         best = t_best;
         out->best = int32_t(out->n_entries);
@@ -1097,9 +1187,11 @@ extern "C" int32_t sq_autotune_nearest_d(sq_ctx* ctx, const sq_bvh* b, const flo
   if (rc) {
     ctx->order = saved_order;
     ctx->blocks_per_sm = saved_bps;
+    ctx->layout = saved_layout;
     return rc;
   }
   ctx->order = out->entries[out->best].order;
   ctx->blocks_per_sm = out->entries[out->best].blocks_per_sm;
+  ctx->layout = out->entries[out->best].layout;
   return finish(ctx);
 }

@@ -48,6 +48,7 @@ struct sq_ctx {
   uint32_t* d_replays = nullptr;  // queries of the last near-first launch answered again in reference order
   sqi::DevBuf replay_list;        // their indices (grown to the largest batch)
   float window = 0x1p-16f;        // relative window past the limit within which near-first still visits nodes
+  int layout = SQ_LAYOUT_BINARY;  // node records of near-first nearest rays (SQ_LAYOUT_*)
   uint64_t launches = 0;
   std::unordered_map<uint64_t, int> occ;  // (kernel, dynamic smem) -> resident blocks per SM
 };
@@ -77,6 +78,11 @@ struct sq_bvh {
   size_t bytes = 0;
   std::vector<uint32_t> h_iidx;  // host node -> interior record (or kNoHit)
   std::vector<uint32_t> h_child_a, h_child_b, h_count;
+  // Four-wide records (WideLayout) built at upload for near-first rays, and
+  // for each of their slots the binary record slot holding the same box.
+  float4* d_wnodes = nullptr;
+  uint32_t* d_wsrc = nullptr;
+  uint32_t n_wide = 0, wroot = 0, wdepth = 0;
   // An f64 scene (sq_bvh_upload_f64): node boxes, node links and leaf
   // parameters in double, answered only by the _f64 entry points.
   int prec = 32;
@@ -146,6 +152,7 @@ inline uint32_t prim_vec(int dim, int narrow) {
 }
 
 inline uint32_t node_vec(int dim) { return (4 * dim + 2 + 3) / 4; }
+inline uint32_t wide_vec(int dim) { return (8 * dim + 4 + 3) / 4; }
 
 inline int32_t arena_reserve(sq_ctx* ctx, size_t bytes) {
   if (ctx->arena.cap >= bytes) return SQ_OK;

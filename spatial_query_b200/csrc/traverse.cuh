@@ -62,6 +62,15 @@ template <int D> struct NodeLayout {
   static constexpr int vec = (words + 3) / 4;
 };
 
+// Four-wide records (the binary tree with every other level folded into its
+// parent): up to four children's boxes, then their codes (kNoHit: an empty
+// slot). Same boxes as the binary records, so the walk prunes exactly the
+// subtrees the binary walk would, in half the dependent fetches.
+template <int D> struct WideLayout {
+  static constexpr int words = 8 * D + 4;  // c0.lo c0.hi ... c3.lo c3.hi code0 .. code3
+  static constexpr int vec = (words + 3) / 4;
+};
+
 template <int D, int N> struct PrimLayout {
   static constexpr int payload = (N == kNarrowAabb)     ? 2 * D
                                  : (N == kNarrowTri)    ? 9
@@ -77,6 +86,8 @@ template <int K> struct QueryLayout {
 
 struct QueryParams {
   const float4* __restrict__ nodes;
+  const float4* __restrict__ wnodes;  // four-wide records (WIDE kernels)
+  uint32_t wroot;                     // the root's four-wide code
   const float4* __restrict__ prims;
   const uint64_t* __restrict__ layers;
   const uint32_t* __restrict__ sub;
@@ -326,14 +337,19 @@ template <int D, int K> struct Lane {
 // at a fixed depth, is searched first; its nearest hit becomes the limit
 // for the rest of the walk from the root, which skips that subtree. The
 // answer is certified exactly as in near-first, so it is the reference's.
-template <int D, int N, int K, bool REF, bool STATS, bool SEED = false>
+// WIDE (near-first nearest rays, no counters, no seed): the walk reads the
+// four-wide records; a step tests up to four children, goes to the nearest
+// and stacks the others farthest first.
+template <int D, int N, int K, bool REF, bool STATS, bool SEED = false, bool WIDE = false>
 __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
+  static_assert(!WIDE || (K == kRayNearest && !REF && !STATS && !SEED), "four-wide walks serve near-first rays only");
   constexpr bool kNearest = (K == kRayNearest || K == kCastNearest);
   constexpr bool kCast = (K == kCastNearest || K == kCastAll);
   constexpr bool kList = (K == kRayAll || K == kCastAll);
   constexpr int QW = kCast ? 4 * D : 2 * D;
   using PL = PrimLayout<D, N>;
   using NL = NodeLayout<D>;
+  using WL = WideLayout<D>;
   constexpr uint32_t FULL = 0xffffffffu;
 
   extern __shared__ uint32_t smem[];
@@ -472,7 +488,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
     L.v_nar = 0;
     L.v_hit = 0;
     L.sp = 0;
-    L.code = p.root_code;
+    L.code = WIDE ? p.wroot : p.root_code;
     float lo[D], hi[D];
 #pragma unroll
     for (int i = 0; i < D; ++i) {
@@ -642,8 +658,55 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
     }
     if (live) {
       bool done = false;
-      // Descend interior child-pair records until a leaf comes up.
+      // Descend interior records until a leaf comes up.
       while (!(L.code & kLeafBit)) {
+        if constexpr (WIDE) {
+          float rec[WL::vec * 4];
+          load_vec<WL::vec>(p.wnodes + size_t(L.code) * WL::vec, rec);
+          float t4[4];
+          uint32_t c4[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            c4[i] = __float_as_uint(rec[8 * D + i]);
+            float te = kInf;
+            if (c4[i] == kNoHit || !test_box(rec + 2 * D * i, rec + 2 * D * i + D, te)) {
+              c4[i] = kNoHit;
+              te = kInf;
+            }
+            t4[i] = te;
+          }
+          // Ascending entry order (a five-comparator network); misses sort last.
+          auto cswap = [&](int a, int b) {
+            if (t4[b] < t4[a]) {
+              const float t = t4[a];
+              t4[a] = t4[b];
+              t4[b] = t;
+              const uint32_t c = c4[a];
+              c4[a] = c4[b];
+              c4[b] = c;
+            }
+          };
+          cswap(0, 1);
+          cswap(2, 3);
+          cswap(0, 2);
+          cswap(1, 3);
+          cswap(1, 2);
+#pragma unroll
+          for (int i = 3; i >= 1; --i) {
+            if (c4[i] != kNoHit) {
+              s_code[L.sp * kThreads + tid] = c4[i];
+              s_t[L.sp * kThreads + tid] = t4[i];
+              ++L.sp;
+            }
+          }
+          if (c4[0] != kNoHit) {
+            L.code = c4[0];
+          } else if (!pop()) {
+            done = true;
+            break;
+          }
+          continue;
+        }
         float rec[NL::vec * 4];
         load_vec<NL::vec>(p.nodes + size_t(L.code) * NL::vec, rec);
         const uint32_t ca = __float_as_uint(rec[4 * D]);
@@ -804,8 +867,23 @@ template <int D, int N> __global__ void __launch_bounds__(256) refit_kernel(cons
 }
 
 // Function-pointer table entry for one (D, narrow) pair.
+// After a refit: every four-wide slot copies its box from the binary record
+// slot that holds the same node's box (src = record << 1 | slot).
+template <int D>
+__global__ void wide_sync_kernel(float4* wnodes, const float4* __restrict__ nodes, const uint32_t* __restrict__ src,
+                                 uint32_t n_slots) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_slots || src[i] == kNoHit) return;
+  const float* from = reinterpret_cast<const float*>(nodes + size_t(src[i] >> 1) * NodeLayout<D>::vec) +
+                      (src[i] & 1u) * 2 * D;
+  float* to = reinterpret_cast<float*>(wnodes + size_t(i / 4) * WideLayout<D>::vec) + (i % 4) * 2 * D;
+  for (int k = 0; k < 2 * D; ++k) to[k] = from[k];
+}
+
 struct KernelSet {
   const void* ray_nearest[2][2];  // [ref][stats]
+  const void* ray_nearest_wide;   // near-first over the four-wide records
+  const void* wide_sync;          // refreshes four-wide boxes from the binary records
   const void* ray_all[2];         // [stats]
   const void* cast_nearest[2];    // [ref]
   const void* cast_all;
@@ -821,6 +899,8 @@ template <int D, int N> KernelSet make_kernel_set() {
   s.ray_nearest[0][1] = (const void*)query_kernel<D, N, kRayNearest, false, true>;
   s.ray_nearest[1][0] = (const void*)query_kernel<D, N, kRayNearest, true, false>;
   s.ray_nearest[1][1] = (const void*)query_kernel<D, N, kRayNearest, true, true>;
+  s.ray_nearest_wide = (const void*)query_kernel<D, N, kRayNearest, false, false, false, true>;
+  s.wide_sync = (const void*)wide_sync_kernel<D>;
   s.ray_all[0] = (const void*)query_kernel<D, N, kRayAll, true, false>;
   s.ray_all[1] = (const void*)query_kernel<D, N, kRayAll, true, true>;
   s.cast_nearest[0] = (const void*)query_kernel<D, N, kCastNearest, false, false>;

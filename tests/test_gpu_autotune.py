@@ -22,7 +22,8 @@ def test_autotune_keeps_hits_exact():
     d_rays = torch.from_numpy(s["rays"]).to(torch.device("cuda", 0))
     torch.cuda.synchronize()
     res = scene.autotune_nearest_d(d_rays, n, s["max_toi"], reps=2)
-    assert len(res["table"]) == 16
+    assert len(res["table"]) == 24  # near-first binary, near-first four-wide, reference: 8 grids each
+    assert {(e["order"], e["layout"]) for e in res["table"]} == {(0, 0), (0, 1), (1, 0)}
     assert all(e["ms"] > 0 for e in res["table"])
     assert res["best"]["ms"] == min(e["ms"] for e in res["table"])
     ref = O.Scene("tris", 3, s["prims"]).nearest(s["rays"], s["max_toi"])
