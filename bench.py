@@ -177,6 +177,21 @@ def cpu_baseline_sample(s, threads: int):
                        f"(Bvh::raycast_nearest_batch_parallel semantics); tree build {build_s:.2f} s not counted")
 
 
+def cpu_rates(run, n_items: int, sample: str, unit: str = "Mrays/s"):
+    """The oracle (the reference CPU path restated) on a bounded sample:
+    `run(threads)` processes `n_items` queries; timed once on every host core
+    (after a warm pass) and once on a single thread."""
+    threads = os.cpu_count() or 1
+    run(threads)
+    out = {}
+    for th in (threads, 1):
+        t0 = time.perf_counter()
+        run(th)
+        out[th] = n_items / (time.perf_counter() - t0) / 1e6
+    base = dict(value=round(out[threads], 4), unit=unit, cores=threads, kind="port", sample=sample)
+    return base, dict(value=round(out[1], 4), unit=unit, cores=1, sample=sample)
+
+
 def f64_delta(s, leaf, toi, threads: int):
     """The GPU's f32 answers against an f64 build of the reference's
     algorithm (the oracle at double precision) on the same f32 inputs."""
@@ -302,6 +317,25 @@ def bench_instanced(args):
         b.synchronize()
     ms = a.elapsed_time(b) / args.frames
     q = nr + nc + no
+    # The CPU path (the oracle's Tlas over its own BLAS trees) on a 1/16 sample
+    # of each query kind of one frame; frames/s scaled from its queries/s.
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    oblas = O.BlasSet(s["blas_offsets"], s["blas_tris"])
+    ot = O.TlasScene("mesh", 3, s["rot"], s["trans"], s["scale"], blas_id=s["blas_id"], blas=oblas)
+    sr, sc_, sg = s["rays"][: nr // 16], s["casts"][: nc // 16], s["regions"][: no // 16]
+    sl = s["cast_len"][: nc // 16]
+
+    def cpu_frame(th):
+        ot.nearest(sr, s["max_toi"], threads=th)
+        ot.shapecast_nearest(sc_, sl, threads=th)
+        ot.overlap(sg, threads=th)
+
+    cpu_all, cpu_one = cpu_rates(cpu_frame, len(sr) + len(sc_) + len(sg),
+                                 "1/16 of one frame's rays, casts and overlap regions (refit not included)",
+                                 unit="Mqueries/s")
+    for c_ in (cpu_all, cpu_one):
+        c_["frames_per_s"] = round(c_["value"] * 1e6 / q, 3)
     line = {"metric": "two-level frames/s: Tlas refit + mixed launch (1,000,000 rays, 262,144 casts, 262,144 overlaps)",
             "value": round(1000.0 / ms, 2), "unit": "frames/s", "n_gpus": 1, "steps": args.frames,
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
@@ -311,6 +345,7 @@ def bench_instanced(args):
                        "queries_per_frame": q, "mqueries_per_s": round(q / ms / 1000.0, 2),
                        "graph": "one CUDA graph per frame (refit + mixed launch)",
                        "gpu_launches_per_frame": int(per_frame_launches)},
+            "cpu_baseline": cpu_all, "cpu_1thread": cpu_one,
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     graph.close()
@@ -346,12 +381,10 @@ def bench_boxes(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     sc = O.Scene("boxes", 3, s["prims"])
-    threads = os.cpu_count() or 1
-    sc.nearest(s["rays"][:4096], s["max_toi"], threads=threads)
-    t0 = time.perf_counter()
-    ref = sc.nearest(s["rays"], s["max_toi"], threads=threads)
-    cpu_s = time.perf_counter() - t0
+    ref = sc.nearest(s["rays"], s["max_toi"])
     same = bool(np.array_equal(ref.leaf, leaf.cpu().numpy().view(np.uint32)))
+    cpu_all, cpu_one = cpu_rates(lambda th: sc.nearest(s["rays"], s["max_toi"], threads=th), n,
+                                 "all 65,536 rays, one pass")
     line = {"metric": "Mrays/s nearest-hit, 10,000 boxes, 65,536 rays", "value": round(n / ms / 1000.0, 3),
             "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -359,8 +392,7 @@ def bench_boxes(args):
             "config": {"workload": "10,000 boxes (centres U[-100,100]^3, half-extents U[0.25,2]); 65,536 rays "
                                    "from a radius-200 sphere toward U[-50,50]^3; t_max 1000",
                        "identical_to_cpu": same, "l2": "flushed between steps"},
-            "cpu_baseline": {"value": round(n / cpu_s / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
-                             "sample": "all 65,536 rays, one pass"},
+            "cpu_baseline": cpu_all, "cpu_1thread": cpu_one,
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     scene.close()
@@ -396,6 +428,14 @@ def bench_mixture(args):
     with ClockSampler(0) as clk:
         r_ms = sum(timed(stream, near, args.steps, flush)) / args.steps
     o_ms = sum(timed(stream, ovl, args.steps, flush)) / args.steps
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    sc = O.Scene("boxes", 6, s["prims"])
+    sr, sg = s["rays"][: n // 16], s["regions"][: no // 16]
+    cpu_all, cpu_one = cpu_rates(lambda th: sc.nearest(sr, s["max_toi"], threads=th), len(sr),
+                                 "1/16 of the rays (65,536), one pass")
+    ov_all, ov_one = cpu_rates(lambda th: sc.overlap(sg, threads=th), len(sg),
+                               "1/16 of the regions (16,384), one pass", unit="Mqueries/s")
     line = {"metric": "Mrays/s nearest-hit, D = 6, 2,097,152 boxes (t_max 2)", "value": round(n / r_ms / 1000.0, 3),
             "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r_ms, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -403,8 +443,10 @@ def bench_mixture(args):
             "config": {"workload": "2,097,152 boxes, centres from a 64-component Gaussian mixture in [0,1]^6, "
                                    "half-extents log-uniform [1e-4, 1e-2]; 1,048,576 rays; 262,144 regions",
                        "overlap": {"value": round(no / o_ms / 1000.0, 3), "unit": "Mqueries/s",
-                                   "ms_per_step": round(o_ms, 4), "leaves_total": int(total)},
+                                   "ms_per_step": round(o_ms, 4), "leaves_total": int(total),
+                                   "cpu_baseline": ov_all, "cpu_1thread": ov_one},
                        "l2": "flushed between steps"},
+            "cpu_baseline": cpu_all, "cpu_1thread": cpu_one,
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     scene.close()
@@ -625,9 +667,21 @@ def main():
     traffic_mlp = profiled_traffic("learned_seeded_terrain.md")
     cpu = None
     f64 = None
+    cpu_one = cpu_all_hits = None
     if rank == 0 and world == 1:
         cpu = cpu_baseline_sample(s, os.cpu_count() or 1)
         f64 = f64_delta(s, d_leaf.cpu().numpy().view(np.uint32), d_toi.cpu().numpy(), os.cpu_count() or 1)
+        # one thread, and the all-hits lists, on 65,536 rays (half of each kind)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        osc = O.Scene("tris", 3, s["prims"])
+        sample = np.ascontiguousarray(np.concatenate([s["rays"][:32768], s["rays"][n // 2: n // 2 + 32768]]))
+        _, cpu_one = cpu_rates(lambda th: osc.nearest(sample, s["max_toi"], threads=th), len(sample),
+                               "65,536 rays (32,768 of each kind), one pass")
+        cpu_all_hits, cpu_all_hits_one = cpu_rates(
+            lambda th: osc.all(sample, s["max_toi"], k=K_ALL, threads=th), len(sample),
+            "65,536 rays (32,768 of each kind), bounded sorted lists k = 16 + full counts")
+        cpu_all_hits["one_thread"] = cpu_all_hits_one["value"]
 
     if rank == 0:
         roof_trav = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -673,7 +727,9 @@ def main():
                                     "reference_best_ms": round(min(e["ms"] for e in tune["table"] if e["order"] == 1), 4)},
                        "all_hits_k16": {"value": round(world * n / (all_ms / 1000) / 1e6, 3), "unit": "Mrays/s",
                                         "ms_per_step": round(all_ms, 4),
-                                        "hits_per_ray": round(float(a_cnt.double().mean().item()), 3)},
+                                        "hits_per_ray": round(float(a_cnt.double().mean().item()), 3),
+                                        "cpu_baseline": cpu_all_hits},
+                       "cpu_1thread": cpu_one,
                        "breakdown_ms": {"inference": round(predict_ms, 4), "seeded_traversal": round(seeded_ms, 4),
                                         "plain_traversal": round(plain_ms, 4)},
                        "nodes_visited_per_ray": {"plain": round(st["nodes_visited"] / n, 3),

@@ -331,7 +331,10 @@ int32_t sq_overlap_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_regions, uin
  * default stream) and returns when the results are written. The first call
  * on a device looks up the array's address on that device: make that first
  * call before any stream capture. Every call shares the one array, so calls
- * that overlap on the GPU (from several threads or streams) race. */
+ * that overlap on the GPU (from several threads or streams) race. With no
+ * sort scratch, each region's leaves are kept ascending by insertion as they
+ * are found: a region with k results costs O(k^2) writes (sq_overlap and
+ * sq_overlap_d append, then sort every segment at once). */
 int32_t sq_overlap_noalloc(const sq_bvh* bvh, const float* d_regions, uint32_t n, const sq_filter* filter,
                            uint64_t* d_offsets, uint32_t* d_leaves, uint64_t leaf_capacity, uint64_t* total,
                            void* stream);

@@ -8,6 +8,7 @@
 // an uploaded scene owns its node and primitive records in HBM.
 #include <cuda_runtime.h>
 
+#include <cub/device/device_segmented_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cuda/std/functional>
 
@@ -710,11 +711,12 @@ int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint3
     p.queries = d_regions;
     p.n = n;
     p.out_count = d_counts;
-    p.fill = 1;
+    p.fill = 2;
     p.csr_offsets = (const unsigned long long*)d_offsets;
     p.csr_leaves = d_leaves;
     int32_t rc = launch_persistent(ctx, b->ks.overlap, p, b->depth, p.n);
     if (rc) return rc;
+    if ((rc = sort_csr_segments(ctx, d_leaves, tot, d_offsets, n))) return rc;
   }
   return SQ_OK;
 }
@@ -1088,6 +1090,30 @@ int32_t sqi::seeded_nearest(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, u
   }
   if ((rc = finish(ctx))) return rc;
   return stats_end(ctx, st);
+}
+
+// Each query's CSR segment of leaves in ascending order: one segmented sort
+// over all segments (the fill pass appends in walk order), with scratch
+// taken from the stream-ordered allocator.
+int32_t sqi::sort_csr_segments(sq_ctx* ctx, uint32_t* d_leaves, uint64_t total, const uint64_t* d_offsets, uint32_t n) {
+  if (total < 2) return SQ_OK;
+  if (total > uint64_t(INT32_MAX)) return fail(ctx, SQ_ERR_CAPACITY, "more than 2^31 overlap results");
+  const auto* beg = reinterpret_cast<const unsigned long long*>(d_offsets);
+  size_t temp_bytes = 0;
+  cub::DoubleBuffer<uint32_t> keys(d_leaves, nullptr);
+  CK(cub::DeviceSegmentedSort::SortKeys(nullptr, temp_bytes, keys, int(total), int(n), beg, beg + 1, ctx->stream));
+  const size_t alt_bytes = (size_t(total) * 4 + 255) & ~size_t(255);
+  char* tmp = nullptr;
+  CK(cudaMallocAsync(reinterpret_cast<void**>(&tmp), alt_bytes + temp_bytes, ctx->stream));
+  keys = cub::DoubleBuffer<uint32_t>(d_leaves, reinterpret_cast<uint32_t*>(tmp));
+  cudaError_t e = cub::DeviceSegmentedSort::SortKeys(tmp + alt_bytes, temp_bytes, keys, int(total), int(n), beg, beg + 1,
+                                                     ctx->stream);
+  if (e == cudaSuccess && keys.Current() != d_leaves)
+    e = cudaMemcpyAsync(d_leaves, keys.Current(), size_t(total) * 4, cudaMemcpyDeviceToDevice, ctx->stream);
+  cudaFreeAsync(tmp, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, "segmented sort of overlap results", e);
+  ctx->launches++;
+  return SQ_OK;
 }
 
 int32_t sqi::near_first_launch(sq_ctx* ctx, const sq_bvh* b, const void* fn, const void* ref_fn, QueryParams& p,

@@ -106,6 +106,10 @@ int32_t near_first_launch(sq_ctx* ctx, const sq_bvh* b, const void* fn, const vo
 constexpr uint32_t kMaxCustomStride = 32;
 int32_t rtc_kernel_set(uint32_t stride, const char* src, KernelSet* out, std::string* log);
 
+// Sorts each CSR segment [offsets[i], offsets[i+1]) of `leaves` ascending
+// (sq_api.cu): the fill passes append in walk order.
+int32_t sort_csr_segments(sq_ctx* ctx, uint32_t* d_leaves, uint64_t total, const uint64_t* d_offsets, uint32_t n);
+
 // Learned-seeded nearest rays (sq_api.cu): enqueues the SEED kernel.
 int32_t seeded_nearest(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, uint32_t n, float max_toi,
                        const int32_t* d_bucket, const uint2* d_buckets, uint32_t n_buckets, const sq_hits& o,

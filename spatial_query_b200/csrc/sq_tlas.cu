@@ -776,6 +776,7 @@ extern "C" int32_t sq_tlas_overlap(sq_ctx* ctx, const sq_tlas* t, const float* r
     q.o_offsets = (const unsigned long long*)(base + o_off);
     q.o_leaves = (uint32_t*)(base + o_lv);
     if ((rc = tlas_run(ctx, t, q, false))) return rc;
+    if ((rc = sort_csr_segments(ctx, (uint32_t*)(base + o_lv), tot, (const uint64_t*)(base + o_off), n))) return rc;
     CK(cudaMemcpyAsync(leaves, base + o_lv, tot * 4, cudaMemcpyDeviceToHost, ctx->stream));
   }
   CK(cudaStreamSynchronize(ctx->stream));

@@ -529,12 +529,8 @@ __global__ void __launch_bounds__(kThreads) tlas_kernel(const TlasParams p) {
           }
           if (hit) {
             if (L.kind == kTOverlapFill) {
-              uint32_t j = L.count;
-              while (j > 0 && p.o_leaves[L.csr_base + j - 1] > id) {
-                p.o_leaves[L.csr_base + j] = p.o_leaves[L.csr_base + j - 1];
-                --j;
-              }
-              p.o_leaves[L.csr_base + j] = id;
+              // appended in walk order; the host call sorts each segment afterwards
+              p.o_leaves[L.csr_base + L.count] = id;
             } else if (L.kind == kTOverlapList) {
               // the first k leaves in ascending order
               const uint32_t k = p.o_k;

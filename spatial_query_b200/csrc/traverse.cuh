@@ -122,7 +122,7 @@ struct QueryParams {
   uint32_t n;
   uint32_t k;
   int crossings;
-  int fill;
+  int fill;  // overlap: 0 count, 1 fill in ascending order, 2 fill in walk order
 };
 
 __device__ __forceinline__ bool accepts(const QueryParams& p, uint32_t id) {
@@ -538,8 +538,12 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
       if (accepts(p, id)) {
         if constexpr (K == kOverlap) {
           if (narrow_overlap<D, N>(rec, L.r.o, L.r.d)) {
-            if (p.fill) {
-              // ascending leaf order within the query's CSR segment
+            if (p.fill == 2) {
+              // appended in walk order; a segmented sort orders each segment afterwards
+              p.csr_leaves[L.csr_base + L.count] = id;
+            } else if (p.fill) {
+              // ascending leaf order within the query's CSR segment, kept by
+              // insertion (the allocation-free path, which has no sort scratch)
               uint32_t j = L.count;
               while (j > 0 && p.csr_leaves[L.csr_base + j - 1] > id) {
                 p.csr_leaves[L.csr_base + j] = p.csr_leaves[L.csr_base + j - 1];
