@@ -1226,28 +1226,50 @@ extern "C" int32_t sq_raycast_nearest_guided(sq_ctx* ctx, const sq_bvh* b, const
   int32_t rc;
   if ((rc = arena_reserve(ctx, cv.off))) return rc;
   char* base = static_cast<char*>(ctx->arena.p);
-  CK(cudaMemcpyAsync(base + o_q, rays, size_t(n) * 24, cudaMemcpyHostToDevice, ctx->stream));
   sq_guide* g = const_cast<sq_guide*>(gc);
-  sq_ctx* saved = g->ctx;
-  g->ctx = ctx;
-  rc = predict(g, reinterpret_cast<const float*>(base + o_q), n, reinterpret_cast<int32_t*>(base + o_b));
-  g->ctx = saved;
-  if (rc) return rc;
   sq_hits dh{};
   dh.leaf = reinterpret_cast<uint32_t*>(base + o_leaf);
   dh.toi = o->toi ? reinterpret_cast<float*>(base + o_toi) : nullptr;
   dh.sub_object = o->sub_object ? reinterpret_cast<uint32_t*>(base + o_sub) : nullptr;
   dh.normal = o->normal ? reinterpret_cast<float*>(base + o_nrm) : nullptr;
   dh.point = o->point ? reinterpret_cast<float*>(base + o_pt) : nullptr;
-  if ((rc = seeded_nearest(ctx, b, reinterpret_cast<const float*>(base + o_q), n, max_toi,
-                           reinterpret_cast<const int32_t*>(base + o_b), g->d_buckets, g->n_buckets, dh, nullptr)))
-    return rc;
-  CK(cudaMemcpyAsync(o->leaf, dh.leaf, size_t(n) * 4, cudaMemcpyDeviceToHost, ctx->stream));
-  if (o->toi) CK(cudaMemcpyAsync(o->toi, dh.toi, size_t(n) * 4, cudaMemcpyDeviceToHost, ctx->stream));
-  if (o->sub_object) CK(cudaMemcpyAsync(o->sub_object, dh.sub_object, size_t(n) * 4, cudaMemcpyDeviceToHost, ctx->stream));
-  if (o->normal) CK(cudaMemcpyAsync(o->normal, dh.normal, size_t(n) * 12, cudaMemcpyDeviceToHost, ctx->stream));
-  if (o->point) CK(cudaMemcpyAsync(o->point, dh.point, size_t(n) * 12, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  const float* d_q = reinterpret_cast<const float*>(base + o_q);
+  int32_t* d_b = reinterpret_cast<int32_t*>(base + o_b);
+  // Chunked: rays of one chunk are copied in and hits of another copied out
+  // while a third is predicted and walked.
+  auto in = [&](uint32_t s0, uint32_t m, cudaStream_t sm) -> int32_t {
+    CK(cudaMemcpyAsync(base + o_q + size_t(s0) * 24, rays + size_t(s0) * 6, size_t(m) * 24, cudaMemcpyHostToDevice,
+                       sm));
+    return SQ_OK;
+  };
+  auto run = [&](uint32_t s0, uint32_t m) -> int32_t {
+    sq_ctx* saved = g->ctx;
+    g->ctx = ctx;
+    int32_t r = predict(g, d_q + size_t(s0) * 6, m, d_b + s0);
+    g->ctx = saved;
+    if (r) return r;
+    sq_hits c = dh;
+    c.leaf += s0;
+    if (c.toi) c.toi += s0;
+    if (c.sub_object) c.sub_object += s0;
+    if (c.normal) c.normal += size_t(s0) * 3;
+    if (c.point) c.point += size_t(s0) * 3;
+    return seeded_nearest(ctx, b, d_q + size_t(s0) * 6, m, max_toi, d_b + s0, g->d_buckets, g->n_buckets, c, nullptr);
+  };
+  auto out = [&](uint32_t s0, uint32_t m, cudaStream_t sm) -> int32_t {
+    auto cp = [&](void* dst, const void* src, size_t per) -> int32_t {
+      if (dst) CK(cudaMemcpyAsync(static_cast<char*>(dst) + size_t(s0) * per,
+                                  static_cast<const char*>(src) + size_t(s0) * per, size_t(m) * per,
+                                  cudaMemcpyDeviceToHost, sm));
+      return SQ_OK;
+    };
+    int32_t r;
+    if ((r = cp(o->leaf, dh.leaf, 4)) || (r = cp(o->toi, dh.toi, 4)) || (r = cp(o->sub_object, dh.sub_object, 4)) ||
+        (r = cp(o->normal, dh.normal, 12)) || (r = cp(o->point, dh.point, 12)))
+      return r;
+    return SQ_OK;
+  };
+  if ((rc = sqi::pipelined(ctx, n, in, run, out))) return rc;
   if (st) *st = sq_query_stats{0, 0, 0, 0};
   return SQ_OK;
 }

@@ -201,6 +201,8 @@ extern "C" int32_t sq_ctx_destroy(sq_ctx* ctx) {
   if (ctx->replay_list.p) cudaFree(ctx->replay_list.p);
   if (ctx->d_counters) cudaFree(ctx->d_counters);
   if (ctx->d_stats) cudaFree(ctx->d_stats);
+  if (ctx->s_in) cudaStreamDestroy(ctx->s_in);
+  if (ctx->s_out) cudaStreamDestroy(ctx->s_out);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
   return SQ_OK;
@@ -777,14 +779,48 @@ int32_t host_nearest(sq_ctx* ctx, const sq_bvh* b, bool cast, const float* q, ui
   size_t o_pt = o->point ? cv.take(size_t(n) * D * 4) : 0;
   if ((rc = arena_reserve(ctx, cv.off))) return rc;
   char* base = (char*)ctx->arena.p;
-  if ((rc = h2d(ctx, base + o_q, q, qb))) return rc;
-  if (mt && (rc = h2d(ctx, base + o_mt, mt, size_t(n) * 4))) return rc;
   sq_hits dh;
   dh.leaf = (uint32_t*)(base + o_leaf);
   dh.toi = o->toi ? (float*)(base + o_toi) : nullptr;
   dh.sub_object = o->sub_object ? (uint32_t*)(base + o_sub) : nullptr;
   dh.normal = o->normal ? (float*)(base + o_nrm) : nullptr;
   dh.point = o->point ? (float*)(base + o_pt) : nullptr;
+  if (!st) {
+    // Chunked: copies in and out overlap the traversal of other chunks.
+    const size_t qw = size_t(cast ? 4 : 2) * D;
+    auto in = [&](uint32_t s0, uint32_t m, cudaStream_t sm) -> int32_t {
+      CK(cudaMemcpyAsync(base + o_q + size_t(s0) * qw * 4, q + size_t(s0) * qw, size_t(m) * qw * 4,
+                         cudaMemcpyHostToDevice, sm));
+      if (mt) CK(cudaMemcpyAsync(base + o_mt + size_t(s0) * 4, mt + s0, size_t(m) * 4, cudaMemcpyHostToDevice, sm));
+      return SQ_OK;
+    };
+    auto run = [&](uint32_t s0, uint32_t m) -> int32_t {
+      sq_hits c = dh;
+      c.leaf += s0;
+      if (c.toi) c.toi += s0;
+      if (c.sub_object) c.sub_object += s0;
+      if (c.normal) c.normal += size_t(s0) * D;
+      if (c.point) c.point += size_t(s0) * D;
+      return nearest_core(ctx, b, cast, (const float*)(base + o_q) + size_t(s0) * qw, m, max_toi,
+                          mt ? (const float*)(base + o_mt) + s0 : nullptr, f, c, false);
+    };
+    auto out = [&](uint32_t s0, uint32_t m, cudaStream_t sm) -> int32_t {
+      auto cp = [&](void* dst, const void* src, size_t per) -> int32_t {
+        if (dst) CK(cudaMemcpyAsync((char*)dst + size_t(s0) * per, (const char*)src + size_t(s0) * per, size_t(m) * per,
+                                    cudaMemcpyDeviceToHost, sm));
+        return SQ_OK;
+      };
+      int32_t r;
+      if ((r = cp(o->leaf, dh.leaf, 4)) || (r = cp(o->toi, dh.toi, 4)) || (r = cp(o->sub_object, dh.sub_object, 4)) ||
+          (r = cp(o->normal, dh.normal, size_t(D) * 4)) || (r = cp(o->point, dh.point, size_t(D) * 4)))
+        return r;
+      return SQ_OK;
+    };
+    if ((rc = pipelined(ctx, n, in, run, out))) return rc;
+    return finish(ctx);
+  }
+  if ((rc = h2d(ctx, base + o_q, q, qb))) return rc;
+  if (mt && (rc = h2d(ctx, base + o_mt, mt, size_t(n) * 4))) return rc;
   if ((rc = stats_begin(ctx, cast ? nullptr : st))) return rc;
   if ((rc = nearest_core(ctx, b, cast, (const float*)(base + o_q), n, max_toi,
                          mt ? (const float*)(base + o_mt) : nullptr, f, dh, st && !cast)))
@@ -1113,6 +1149,55 @@ int32_t sqi::sort_csr_segments(sq_ctx* ctx, uint32_t* d_leaves, uint64_t total, 
   cudaFreeAsync(tmp, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, "segmented sort of overlap results", e);
   ctx->launches++;
+  return SQ_OK;
+}
+
+uint32_t sqi::pipeline_chunks(uint32_t n) {
+  // Chunks of at least 262,144 queries: below that the launch tails cost
+  // more than the copies they hide.
+  if (n >= 1u << 20) return 4;
+  if (n >= 1u << 19) return 2;
+  return 1;
+}
+
+int32_t sqi::pipelined(sq_ctx* ctx, uint32_t n, const std::function<int32_t(uint32_t, uint32_t, cudaStream_t)>& in,
+                       const std::function<int32_t(uint32_t, uint32_t)>& run,
+                       const std::function<int32_t(uint32_t, uint32_t, cudaStream_t)>& out) {
+  const uint32_t k = pipeline_chunks(n);
+  int32_t rc;
+  if (k == 1) {
+    if ((rc = in(0, n, ctx->stream)) || (rc = run(0, n)) || (rc = out(0, n, ctx->stream))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SQ_OK;
+  }
+  if (!ctx->s_in) CK(cudaStreamCreateWithFlags(&ctx->s_in, cudaStreamNonBlocking));
+  if (!ctx->s_out) CK(cudaStreamCreateWithFlags(&ctx->s_out, cudaStreamNonBlocking));
+  std::vector<cudaEvent_t> ev(2 * k + 1, nullptr);
+  for (auto& e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  // The copies in start after whatever the context's stream holds (earlier
+  // calls may still be reading the scratch buffers).
+  rc = SQ_OK;
+  cudaError_t ce = cudaEventRecord(ev[2 * k], ctx->stream);
+  if (ce == cudaSuccess) ce = cudaStreamWaitEvent(ctx->s_in, ev[2 * k], 0);
+  const uint32_t step = (n + k - 1) / k;
+  for (uint32_t c = 0; c < k && rc == SQ_OK && ce == cudaSuccess; ++c) {
+    const uint32_t s0 = c * step, m = std::min(step, n - s0);
+    if ((rc = in(s0, m, ctx->s_in))) break;
+    if ((ce = cudaEventRecord(ev[2 * c], ctx->s_in)) != cudaSuccess) break;
+    if ((ce = cudaStreamWaitEvent(ctx->stream, ev[2 * c], 0)) != cudaSuccess) break;
+    if ((rc = run(s0, m))) break;
+    if ((ce = cudaEventRecord(ev[2 * c + 1], ctx->stream)) != cudaSuccess) break;
+    if ((ce = cudaStreamWaitEvent(ctx->s_out, ev[2 * c + 1], 0)) != cudaSuccess) break;
+    rc = out(s0, m, ctx->s_out);
+  }
+  // Every stream settles before the events go and before an error returns.
+  cudaStreamSynchronize(ctx->s_in);
+  cudaStreamSynchronize(ctx->stream);
+  const cudaError_t se = cudaStreamSynchronize(ctx->s_out);
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (rc) return rc;
+  if (ce != cudaSuccess) return cuda_fail(ctx, "chunked host-buffer call", ce);
+  if (se != cudaSuccess) return cuda_fail(ctx, "chunked host-buffer call", se);
   return SQ_OK;
 }
 
