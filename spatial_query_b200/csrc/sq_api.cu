@@ -680,15 +680,47 @@ size_t overlap_scan_temp(uint32_t n) {
   return temp;
 }
 
+// Scratch of overlap_core: per-region counts, the heavy-region list and
+// flags, their counter, then the scan's temporary storage.
+size_t overlap_scratch_bytes(uint32_t n) {
+  const auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+  return al((size_t(n) + 1) * 4) + al(size_t(n) * 4 + 4) + al(size_t(n) + 1) + al(16) + overlap_scan_temp(n) + 256;
+}
+
+// Records a region may visit before the warp-per-region kernel takes it.
+constexpr uint32_t kOverlapVisitBudget = 256;
+
+// Launches overlap_heavy_kernel over the regions the count pass listed.
+int32_t launch_heavy(sq_ctx* ctx, const sq_bvh* b, QueryParams& p) {
+  const uint32_t cap = 64u * (b->depth + 1);
+  p.stack = int(cap);
+  const size_t smem = size_t(kHeavyWarps) * cap * 4;
+  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(b->ks.overlap_heavy, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  void* args[] = {&p};
+  CK(cudaLaunchKernel(b->ks.overlap_heavy, dim3(ctx->sm_count * 4), dim3(32 * kHeavyWarps), args, smem, ctx->stream));
+  ctx->launches++;
+  return SQ_OK;
+}
+
 int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint32_t n, const sq_filter* f,
                      uint64_t* d_offsets, uint32_t* d_leaves, uint64_t cap, uint64_t* total, void* scratch,
                      size_t scratch_bytes) {
   if (!b->ks.overlap) return fail(ctx, SQ_ERR_UNSUPPORTED, "this scene's narrow phase has no overlap query");
-  uint32_t* d_counts = (uint32_t*)scratch;
-  size_t counts_bytes = ((size_t(n) + 1) * 4 + 255) & ~size_t(255);
-  void* temp = (char*)scratch + counts_bytes;
-  size_t temp_bytes = scratch_bytes - counts_bytes;
+  const auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
+  Carve sc;
+  const size_t o_cnt = sc.take((size_t(n) + 1) * 4), o_hl = sc.take(size_t(n) * 4 + 4), o_hf = sc.take(size_t(n) + 1),
+               o_hc = sc.take(16);
+  (void)al;
+  uint32_t* d_counts = (uint32_t*)((char*)scratch + o_cnt);
+  uint32_t* d_hlist = (uint32_t*)((char*)scratch + o_hl);
+  uint8_t* d_hflag = (uint8_t*)((char*)scratch + o_hf);
+  uint32_t* d_hcount = (uint32_t*)((char*)scratch + o_hc);
+  void* temp = (char*)scratch + sc.off;
+  size_t temp_bytes = scratch_bytes - sc.off;
   CK(cudaMemsetAsync(d_counts, 0, size_t(n + 1) * 4, ctx->stream));
+  CK(cudaMemsetAsync(d_hflag, 0, size_t(n) + 1, ctx->stream));
+  CK(cudaMemsetAsync(d_hcount, 0, 4, ctx->stream));
+  const bool heavy = b->ks.overlap_heavy != nullptr;
   if (b->n_nodes != 0 && n != 0) {
     QueryParams p;
     base_params(b, f, p);
@@ -696,15 +728,25 @@ int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint3
     p.n = n;
     p.out_count = d_counts;
     p.fill = 0;
+    if (heavy) {
+      p.heavy_list = d_hlist;
+      p.heavy_count = d_hcount;
+      p.heavy_flag = d_hflag;
+      p.visit_budget = kOverlapVisitBudget;
+    }
     int32_t rc = launch_persistent(ctx, b->ks.overlap, p, b->depth, p.n);
     if (rc) return rc;
+    if (heavy && (rc = launch_heavy(ctx, b, p))) return rc;
   }
   CK(cub::DeviceScan::ExclusiveScan(temp, temp_bytes, d_counts, (unsigned long long*)d_offsets, cuda::std::plus<>{},
                                     0ull, int(n) + 1, ctx->stream));
   ctx->launches++;
   unsigned long long tot = 0;
+  uint32_t hc = 0;
   CK(cudaMemcpyAsync(&tot, d_offsets + n, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(&hc, d_hcount, 4, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  if (hc & 0x80000000u) return fail(ctx, SQ_ERR_CAPACITY, "overlap: a heavy region's node stack overflowed");
   if (total) *total = tot;
   if (tot > cap) return fail(ctx, SQ_ERR_CAPACITY, "overlap results exceed leaf_capacity");
   if (tot && b->n_nodes != 0) {
@@ -716,8 +758,14 @@ int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint3
     p.fill = 2;
     p.csr_offsets = (const unsigned long long*)d_offsets;
     p.csr_leaves = d_leaves;
+    if (heavy) {
+      p.heavy_list = d_hlist;
+      p.heavy_count = d_hcount;
+      p.heavy_flag = d_hflag;
+    }
     int32_t rc = launch_persistent(ctx, b->ks.overlap, p, b->depth, p.n);
     if (rc) return rc;
+    if (heavy && hc && (rc = launch_heavy(ctx, b, p))) return rc;
     if ((rc = sort_csr_segments(ctx, d_leaves, tot, d_offsets, n))) return rc;
   }
   return SQ_OK;
@@ -731,7 +779,7 @@ extern "C" int32_t sq_overlap_d(sq_ctx* ctx, const sq_bvh* b, const float* d_reg
   int32_t rc = check_scene(ctx, b);
   if (rc) return rc;
   if (!d_offsets || (n && !d_regions)) return fail(ctx, SQ_ERR_INVALID, "null argument");
-  size_t need = ((size_t(n) + 1) * 4 + 255 & ~size_t(255)) + overlap_scan_temp(n) + 256;
+  size_t need = overlap_scratch_bytes(n);
   if ((rc = arena_reserve(ctx, need))) return rc;
   if ((rc = overlap_core(ctx, b, d_regions, n, f, d_offsets, d_leaves, cap, total, ctx->arena.p, need))) return rc;
   if ((rc = finish(ctx))) return rc;
@@ -921,7 +969,7 @@ extern "C" int32_t sq_overlap(sq_ctx* ctx, const sq_bvh* b, const float* regions
   if (!offsets || (n && !regions)) return fail(ctx, SQ_ERR_INVALID, "null argument");
   const int D = b->dim;
   const size_t rb = size_t(n) * 2 * D * 4;
-  const size_t scan = ((size_t(n) + 1) * 4 + 255 & ~size_t(255)) + overlap_scan_temp(n) + 256;
+  const size_t scan = overlap_scratch_bytes(n);
   Carve cv;
   size_t o_r = cv.take(rb), o_off = cv.take((size_t(n) + 1) * 8), o_lv = cv.take(std::max<uint64_t>(cap, 1) * 4);
   size_t o_scr = cv.take(scan);

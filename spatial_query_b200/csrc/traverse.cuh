@@ -123,6 +123,13 @@ struct QueryParams {
   uint32_t k;
   int crossings;
   int fill;  // overlap: 0 count, 1 fill in ascending order, 2 fill in walk order
+  // Overlap regions that visit more than visit_budget records in the count
+  // pass are left to overlap_heavy_kernel (a warp per region): listed in
+  // heavy_list, flagged in heavy_flag (the fill pass skips them).
+  uint32_t* heavy_list;
+  uint32_t* heavy_count;
+  uint8_t* heavy_flag;
+  uint32_t visit_budget;
 };
 
 __device__ __forceinline__ bool accepts(const QueryParams& p, uint32_t id) {
@@ -483,6 +490,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
     L.csr_base = 0;
     if constexpr (K == kOverlap) {
       if (p.fill) L.csr_base = p.csr_offsets[q];
+      if (p.fill && p.heavy_flag && p.heavy_flag[q]) return false;  // filled by the warp-per-region kernel
     }
     L.v_nodes = STATS ? 1u : 0u;
     L.v_nar = 0;
@@ -719,6 +727,16 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
         const bool pa = test_box(rec, rec + D, ta) && (!SEED || ca != L.skip);
         const bool pb = test_box(rec + 2 * D, rec + 3 * D, tb) && (!SEED || cb != L.skip);
         if (STATS) L.v_nodes += 2;
+        if constexpr (K == kOverlap) {
+          // A region heavier than the budget goes to the warp-per-region
+          // kernel instead of holding the launch's tail on one thread.
+          if (p.heavy_list && !p.fill && ++L.v_nar > p.visit_budget) {
+            p.heavy_flag[L.q] = 1;
+            p.heavy_list[atomicAdd(p.heavy_count, 1u)] = L.q;
+            done = true;
+            break;
+          }
+        }
         if (pa && pb) {
           // Reference order: child_a waits, child_b goes first. Near-first:
           // the smaller entry goes first.
@@ -759,6 +777,104 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
       atomicAdd(p.stats + 2, c_nar);
       atomicAdd(p.stats + 3, c_hit);
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Heavy overlap regions: one warp per region. The warp keeps the region's
+// pending nodes in a shared-memory stack and each step takes up to 32 of them
+// from the top, one per lane: an interior record's overlapping children are
+// pushed (warp prefix sum for the slots), a leaf's accepted overlapping
+// primitives are counted (count pass) or written to the region's CSR segment
+// in any order (fill pass; the segmented sort that follows orders them).
+// Any order of visits finds the same set of leaves as the crate's walk.
+// Stack: each step replaces the <= 32 entries it takes with <= 64 children one
+// level deeper, so at most 32 entries per level stay below the top: the
+// stack never holds more than 32 x (depth + 1) + 32 entries; it is sized
+// 64 x (depth + 1) per warp (dynamic shared memory), and a push past it is
+// refused and reported through heavy_count's high bit instead of written.
+// ---------------------------------------------------------------------------
+constexpr int kHeavyWarps = 4;
+
+template <int D, int N>
+__global__ void __launch_bounds__(32 * kHeavyWarps) overlap_heavy_kernel(const QueryParams p) {
+  using PL = PrimLayout<D, N>;
+  using NL = NodeLayout<D>;
+  constexpr uint32_t FULL = 0xffffffffu;
+  extern __shared__ uint32_t heavy_smem[];
+  __shared__ unsigned long long s_fill[kHeavyWarps];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cap = p.stack;  // entries per warp
+  uint32_t* stk = heavy_smem + size_t(w) * cap;
+  const uint32_t nh = *p.heavy_count & 0x7FFFFFFFu;
+  for (uint32_t i = blockIdx.x * kHeavyWarps + w; i < nh; i += gridDim.x * kHeavyWarps) {
+    const uint32_t q = p.heavy_list[i];
+    float lo[D], hi[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      lo[k] = p.queries[size_t(q) * 2 * D + k];
+      hi[k] = p.queries[size_t(q) * 2 * D + D + k];
+    }
+    if (lane == 0) s_fill[w] = p.fill ? p.csr_offsets[q] : 0ull;
+    uint32_t count = 0;
+    int sp = 0;
+    if (box_overlap<D>(p.root_box, p.root_box + D, lo, hi)) {
+      if (lane == 0) stk[0] = p.root_code;
+      sp = 1;
+    }
+    __syncwarp();
+    while (sp > 0) {
+      const int take = sp < 32 ? sp : 32;
+      const uint32_t code = lane < take ? stk[sp - take + lane] : kNoHit;
+      __syncwarp();
+      sp -= take;
+      uint32_t push[2] = {kNoHit, kNoHit};
+      if (code != kNoHit) {
+        if (code & kLeafBit) {
+          uint32_t pos = code & ~kLeafBit;
+          for (;;) {
+            float rec[PL::vec * 4];
+            load_vec<PL::vec>(p.prims + size_t(pos) * PL::vec, rec);
+            const uint32_t idw = __float_as_uint(rec[PL::id_word]);
+            const uint32_t id = idw & ~kLeafBit;
+            if (accepts(p, id) && narrow_overlap<D, N>(rec, lo, hi)) {
+              if (p.fill) p.csr_leaves[atomicAdd(&s_fill[w], 1ull)] = id;
+              else ++count;
+            }
+            if (idw & kLeafBit) break;
+            ++pos;
+          }
+        } else {
+          float rec[NL::vec * 4];
+          load_vec<NL::vec>(p.nodes + size_t(code) * NL::vec, rec);
+          if (box_overlap<D>(rec, rec + D, lo, hi)) push[0] = __float_as_uint(rec[4 * D]);
+          if (box_overlap<D>(rec + 2 * D, rec + 3 * D, lo, hi)) push[1] = __float_as_uint(rec[4 * D + 1]);
+        }
+      }
+      const int mine = (push[0] != kNoHit) + (push[1] != kNoHit);
+      int incl = mine;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const int total = __shfl_sync(FULL, incl, 31);
+      int at = sp + incl - mine;
+      for (int k = 0; k < 2; ++k) {
+        if (push[k] == kNoHit) continue;
+        if (at < cap) stk[at] = push[k];
+        else atomicOr(p.heavy_count, 0x80000000u);  // refused: reported to the host
+        ++at;
+      }
+      sp = min(sp + total, cap);
+      __syncwarp();
+    }
+    if (!p.fill) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) count += __shfl_down_sync(FULL, count, o);
+      if (lane == 0) p.out_count[q] = count;
+    }
+    __syncwarp();
   }
 }
 
@@ -892,6 +1008,7 @@ struct KernelSet {
   const void* cast_nearest[2];    // [ref]
   const void* cast_all;
   const void* overlap;
+  const void* overlap_heavy;  // warp-per-region overlap of the regions over the visit budget
   const void* refit_leaves;
   const void* ray_nearest_seeded[2];  // [stats]; D = 3 only
 };
@@ -911,6 +1028,7 @@ template <int D, int N> KernelSet make_kernel_set() {
   s.cast_nearest[1] = (const void*)query_kernel<D, N, kCastNearest, true, false>;
   s.cast_all = (const void*)query_kernel<D, N, kCastAll, true, false>;
   s.overlap = (const void*)query_kernel<D, N, kOverlap, true, false>;
+  s.overlap_heavy = (const void*)overlap_heavy_kernel<D, N>;
   s.refit_leaves = (const void*)refit_kernel<D, N>;
   s.ray_nearest_seeded[0] = nullptr;
   s.ray_nearest_seeded[1] = nullptr;
