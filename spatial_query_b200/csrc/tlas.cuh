@@ -302,8 +302,13 @@ template <int D> struct TLane {
   uint32_t v_nodes, v_nar, v_hit;
 };
 
+// The mesh-instance walk (the two-level benchmark's kernel) is latency-bound
+// with divergent lanes, so resident warps count more than registers: it is
+// held to six resident blocks per SM (80 registers, a few spilled), which
+// measured 7.1 ms per million rays against 8.8 ms at its natural 112.
 template <int D, int IK, bool REF, bool STATS>
-__global__ void __launch_bounds__(kThreads) tlas_kernel(const TlasParams p) {
+__global__ void __launch_bounds__(kThreads, (IK == kInstMesh && !REF && !STATS) ? 6 : 1)
+    tlas_kernel(const TlasParams p) {
   using IL = InstLayout<D, IK>;
   using NL = NodeLayout<D>;
   constexpr uint32_t FULL = 0xffffffffu;
