@@ -364,7 +364,10 @@ class Context:
         self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown may already have torn down the ctypes handles
+            pass
 
     def check(self, rc: int, what: str):
         if rc:
@@ -430,7 +433,10 @@ class Graph:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown may already have torn down the ctypes handles
+            pass
 
 
 @dataclass
@@ -536,7 +542,10 @@ class DeviceBvh:
         self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown may already have torn down the ctypes handles
+            pass
 
     def info(self) -> dict:
         i = _Info()
@@ -710,7 +719,10 @@ class DeviceBvh64:
         self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown may already have torn down the ctypes handles
+            pass
 
     def raycast_nearest(self, rays, max_toi, mask=None, exclude=None, stats=False) -> Hits:
         """rays: [n, 2D] doubles; max_toi a scalar or one per ray."""
@@ -831,7 +843,10 @@ class BlasSet:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown may already have torn down the ctypes handles
+            pass
 
 
 def instance_world_aabbs(kind: str, dim: int, rot, trans, param, blas_id=None, blas: BlasSet | None = None):
@@ -877,7 +892,10 @@ class DeviceTlas:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown may already have torn down the ctypes handles
+            pass
 
     def refit(self, trans, rot=None, param=None):
         self.trans = _f32(trans)
@@ -1014,7 +1032,10 @@ class Guide:
         self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown may already have torn down the ctypes handles
+            pass
 
     def info(self) -> dict:
         i = _GuideInfo()
