@@ -11,6 +11,7 @@
 
 #ifdef __CUDACC_RTC__
 // Runtime compilation (NVRTC, for consumer narrow phases) has no <cstdint>.
+typedef unsigned char uint8_t;
 typedef unsigned int uint32_t;
 typedef int int32_t;
 typedef unsigned long long uint64_t;
