@@ -378,6 +378,7 @@ def bench_boxes(args):
     torch.cuda.synchronize()
     with ClockSampler(0) as clk:
         ms = sum(timed(stream, near, args.steps, flush)) / args.steps
+    learned = learned_boxes(args, scene, ctx, stream, flush, s, d_rays, leaf, toi, ms)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     sc = O.Scene("boxes", 3, s["prims"])
@@ -391,12 +392,75 @@ def bench_boxes(args):
             "data": "synthetic (seeded boxes and rays)",
             "config": {"workload": "10,000 boxes (centres U[-100,100]^3, half-extents U[0.25,2]); 65,536 rays "
                                    "from a radius-200 sphere toward U[-50,50]^3; t_max 1000",
-                       "identical_to_cpu": same, "l2": "flushed between steps"},
+                       "identical_to_cpu": same, "l2": "flushed between steps", "learned_guide": learned},
             "cpu_baseline": cpu_all, "cpu_1thread": cpu_one,
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     scene.close()
     ctx.close()
+
+
+def learned_boxes(args, scene, ctx, stream, flush, s, d_rays, leaf, toi, plain_ms):
+    """The learned guide on the 10,000-box scene and its 65,536 rays: trained
+    on rays of the same distribution (another seed) labelled by the plain
+    traversal, then timed against the plain query (ms `plain_ms`), with node
+    visits per ray and the hit agreement. The buckets are the subtrees at the
+    deepest level that gives at most 4,096 of them."""
+    import torch
+    import spatial_query_b200 as sq
+    from spatial_query_b200 import scenes
+    dev = d_rays.device
+    n = d_rays.shape[0]
+    guide, depth = None, min(24, scene.info()["max_depth"])
+    while guide is None:
+        try:
+            guide = sq.Guide(scene, depth=depth, seed=0)
+        except sq.SqError:
+            depth -= 1
+    gi = guide.info()
+    t0 = time.perf_counter()
+    n_train = args.train_rays
+    d_train = torch.from_numpy(scenes.sphere_rays(scenes.Rng(5), n_train, 3)).to(dev)
+    d_lab = torch.empty(n_train, dtype=torch.int32, device=dev)
+    guide.label_d(d_train, n_train, s["max_toi"], d_lab)
+    losses = guide.train_d(d_train, d_lab, n_train, args.epochs)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    del d_train, d_lab
+    g_leaf, g_toi = torch.empty_like(leaf), torch.empty_like(toi)
+    d_bucket = torch.empty(n, dtype=torch.int32, device=dev)
+    guided = lambda: guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], g_leaf, g_toi)
+    predict = lambda: guide.predict_d(d_rays, n, d_bucket)
+    seeded = lambda: guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], g_leaf, g_toi, d_bucket=d_bucket)
+    st = scene.raycast_nearest_d(d_rays, n, s["max_toi"], leaf, toi, stats=True)
+    predict()
+    st_g = guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], g_leaf, g_toi, d_bucket=d_bucket, stats=True)
+    d_lt = torch.empty(n, dtype=torch.int32, device=dev)
+    guide.label_d(d_rays, n, s["max_toi"], d_lt)
+    torch.cuda.synchronize()
+    agree = float((g_leaf == leaf).float().mean().item())
+    identical = bool(torch.equal(g_leaf, leaf) and torch.equal(g_toi.view(torch.int32), toi.view(torch.int32)))
+    if not identical:
+        raise SystemExit("learned-seeded hits differ from the plain query's")
+    hit = d_lt >= 0
+    top1 = float((d_bucket[hit] == d_lt[hit]).float().mean().item())
+    for _ in range(args.warmup):
+        guided()
+    torch.cuda.synchronize()
+    g_ms = sum(timed(stream, guided, args.steps, flush)) / args.steps
+    pr_ms = sum(timed(stream, predict, args.steps, flush)) / args.steps
+    sd_ms = sum(timed(stream, seeded, args.steps, flush)) / args.steps
+    guide.close()
+    return {"value": round(n / g_ms / 1000.0, 3), "unit": "Mrays/s", "ms_per_step": round(g_ms, 4),
+            "learned_vs_plain": round(plain_ms / g_ms, 4), "hit_id_agreement": agree, "identical_hits": identical,
+            "inference_ms": round(pr_ms, 4), "seeded_traversal_ms": round(sd_ms, 4),
+            "inference_tflops": round(2 * (MLP_MACS - 128 * (4096 - gi["n_out"])) * n / (pr_ms / 1000) / 1e12, 1),
+            "nodes_visited_per_ray": {"plain": round(st["nodes_visited"] / n, 2),
+                                      "seeded": round(st_g["nodes_visited"] / n, 2)},
+            "buckets": gi["n_buckets"], "outputs": gi["n_out"], "bucket_depth": depth, "top1_accuracy": round(top1, 4),
+            "training": {"rays": n_train, "epochs": args.epochs, "batch": 8192, "optimizer": "AdamW lr 1e-3",
+                         "seconds": round(train_s, 2), "final_loss": round(float(losses[-1]), 4),
+                         "rays_from": "the same sphere-to-box distribution, seed 5"}}
 
 
 def bench_mixture(args):

@@ -117,12 +117,18 @@ def boxes_scene(seed: int = 0, n_boxes: int = 10_000, n_rays: int = 65_536, dim:
     c = f32_range(raw[:, :dim], -100.0, 100.0)
     h = f32_range(raw[:, dim:], 0.25, 2.0)
     prims = np.ascontiguousarray(np.concatenate([c - h, c + h], axis=1), dtype=np.float32)
+    rays = sphere_rays(rng, n_rays, dim)
+    return dict(name=f"boxes{dim}d", dim=dim, kind="boxes", prims=prims, rays=rays, max_toi=1000.0)
+
+
+def sphere_rays(rng: Rng, n_rays: int, dim: int = 3) -> np.ndarray:
+    """The boxes scene's rays: origins uniform on the radius-200 sphere,
+    directions normalised toward points U[-50,50]^D."""
     sph = rng.normal64((n_rays, dim))
     sph /= np.linalg.norm(sph, axis=1, keepdims=True)
     origins = (200.0 * sph).astype(np.float32)
     targets = rng.range(-50.0, 50.0, (n_rays, dim))
-    rays = rays_from(origins, targets - origins)
-    return dict(name=f"boxes{dim}d", dim=dim, kind="boxes", prims=prims, rays=rays, max_toi=1000.0)
+    return rays_from(origins, targets - origins)
 
 
 # ---------------------------------------------------------------------------
