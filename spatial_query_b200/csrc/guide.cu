@@ -1242,9 +1242,9 @@ extern "C" int32_t sq_raycast_nearest_guided(sq_ctx* ctx, const sq_bvh* b, const
                        sm));
     return SQ_OK;
   };
-  auto run = [&](uint32_t s0, uint32_t m) -> int32_t {
+  auto run = [&](sq_ctx* lane, uint32_t s0, uint32_t m) -> int32_t {
     sq_ctx* saved = g->ctx;
-    g->ctx = ctx;
+    g->ctx = lane;
     int32_t r = predict(g, d_q + size_t(s0) * 6, m, d_b + s0);
     g->ctx = saved;
     if (r) return r;
@@ -1254,7 +1254,7 @@ extern "C" int32_t sq_raycast_nearest_guided(sq_ctx* ctx, const sq_bvh* b, const
     if (c.sub_object) c.sub_object += s0;
     if (c.normal) c.normal += size_t(s0) * 3;
     if (c.point) c.point += size_t(s0) * 3;
-    return seeded_nearest(ctx, b, d_q + size_t(s0) * 6, m, max_toi, d_b + s0, g->d_buckets, g->n_buckets, c, nullptr);
+    return seeded_nearest(lane, b, d_q + size_t(s0) * 6, m, max_toi, d_b + s0, g->d_buckets, g->n_buckets, c, nullptr);
   };
   auto out = [&](uint32_t s0, uint32_t m, cudaStream_t sm) -> int32_t {
     auto cp = [&](void* dst, const void* src, size_t per) -> int32_t {
@@ -1269,6 +1269,15 @@ extern "C" int32_t sq_raycast_nearest_guided(sq_ctx* ctx, const sq_bvh* b, const
       return r;
     return SQ_OK;
   };
+  // The weight images are refreshed once, on the context's stream, before
+  // either lane predicts from them.
+  {
+    sq_ctx* saved = g->ctx;
+    g->ctx = ctx;
+    rc = refresh_images(g);
+    g->ctx = saved;
+    if (rc) return rc;
+  }
   if ((rc = sqi::pipelined(ctx, n, in, run, out))) return rc;
   if (st) *st = sq_query_stats{0, 0, 0, 0};
   return SQ_OK;

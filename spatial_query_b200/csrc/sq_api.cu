@@ -196,6 +196,7 @@ extern "C" int32_t sq_ctx_destroy(sq_ctx* ctx) {
   if (!ctx) return SQ_OK;
   cudaSetDevice(ctx->device);
   if (ctx->own) cudaStreamSynchronize(ctx->own);
+  if (ctx->lane) sq_ctx_destroy(ctx->lane);
   if (ctx->arena.p) cudaFree(ctx->arena.p);
   if (ctx->d_replays) cudaFree(ctx->d_replays);
   if (ctx->replay_list.p) cudaFree(ctx->replay_list.p);
@@ -842,14 +843,14 @@ int32_t host_nearest(sq_ctx* ctx, const sq_bvh* b, bool cast, const float* q, ui
       if (mt) CK(cudaMemcpyAsync(base + o_mt + size_t(s0) * 4, mt + s0, size_t(m) * 4, cudaMemcpyHostToDevice, sm));
       return SQ_OK;
     };
-    auto run = [&](uint32_t s0, uint32_t m) -> int32_t {
+    auto run = [&](sq_ctx* lane, uint32_t s0, uint32_t m) -> int32_t {
       sq_hits c = dh;
       c.leaf += s0;
       if (c.toi) c.toi += s0;
       if (c.sub_object) c.sub_object += s0;
       if (c.normal) c.normal += size_t(s0) * D;
       if (c.point) c.point += size_t(s0) * D;
-      return nearest_core(ctx, b, cast, (const float*)(base + o_q) + size_t(s0) * qw, m, max_toi,
+      return nearest_core(lane, b, cast, (const float*)(base + o_q) + size_t(s0) * qw, m, max_toi,
                           mt ? (const float*)(base + o_mt) + s0 : nullptr, f, c, false);
     };
     auto out = [&](uint32_t s0, uint32_t m, cudaStream_t sm) -> int32_t {
@@ -1209,41 +1210,62 @@ uint32_t sqi::pipeline_chunks(uint32_t n) {
 }
 
 int32_t sqi::pipelined(sq_ctx* ctx, uint32_t n, const std::function<int32_t(uint32_t, uint32_t, cudaStream_t)>& in,
-                       const std::function<int32_t(uint32_t, uint32_t)>& run,
+                       const std::function<int32_t(sq_ctx*, uint32_t, uint32_t)>& run,
                        const std::function<int32_t(uint32_t, uint32_t, cudaStream_t)>& out) {
   const uint32_t k = pipeline_chunks(n);
   int32_t rc;
   if (k == 1) {
-    if ((rc = in(0, n, ctx->stream)) || (rc = run(0, n)) || (rc = out(0, n, ctx->stream))) return rc;
+    if ((rc = in(0, n, ctx->stream)) || (rc = run(ctx, 0, n)) || (rc = out(0, n, ctx->stream))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     return SQ_OK;
   }
   if (!ctx->s_in) CK(cudaStreamCreateWithFlags(&ctx->s_in, cudaStreamNonBlocking));
   if (!ctx->s_out) CK(cudaStreamCreateWithFlags(&ctx->s_out, cudaStreamNonBlocking));
-  std::vector<cudaEvent_t> ev(2 * k + 1, nullptr);
+  if (!ctx->lane) {
+    sq_ctx* l = nullptr;
+    if ((rc = sq_ctx_create(ctx->device, &l))) return fail(ctx, rc, "second compute lane");
+    ctx->lane = l;
+  }
+  sq_ctx* lane = ctx->lane;
+  lane->order = ctx->order;
+  lane->blocks_per_sm = ctx->blocks_per_sm;
+  lane->window = ctx->window;
+  lane->layout = ctx->layout;
+  const uint64_t lane_launches = lane->launches;
+  std::vector<cudaEvent_t> ev(2 * k + 2, nullptr);
   for (auto& e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  // The copies in start after whatever the context's stream holds (earlier
-  // calls may still be reading the scratch buffers).
+  // The copies in and the second lane start after whatever the context's
+  // stream holds (earlier calls may still be reading the scratch buffers).
   rc = SQ_OK;
+  sq_ctx* failed = ctx;
   cudaError_t ce = cudaEventRecord(ev[2 * k], ctx->stream);
   if (ce == cudaSuccess) ce = cudaStreamWaitEvent(ctx->s_in, ev[2 * k], 0);
+  if (ce == cudaSuccess) ce = cudaStreamWaitEvent(lane->stream, ev[2 * k], 0);
   const uint32_t step = (n + k - 1) / k;
   for (uint32_t c = 0; c < k && rc == SQ_OK && ce == cudaSuccess; ++c) {
     const uint32_t s0 = c * step, m = std::min(step, n - s0);
+    sq_ctx* on = (c & 1) ? lane : ctx;
     if ((rc = in(s0, m, ctx->s_in))) break;
     if ((ce = cudaEventRecord(ev[2 * c], ctx->s_in)) != cudaSuccess) break;
-    if ((ce = cudaStreamWaitEvent(ctx->stream, ev[2 * c], 0)) != cudaSuccess) break;
-    if ((rc = run(s0, m))) break;
-    if ((ce = cudaEventRecord(ev[2 * c + 1], ctx->stream)) != cudaSuccess) break;
+    if ((ce = cudaStreamWaitEvent(on->stream, ev[2 * c], 0)) != cudaSuccess) break;
+    if ((rc = run(on, s0, m))) {
+      failed = on;
+      break;
+    }
+    if ((ce = cudaEventRecord(ev[2 * c + 1], on->stream)) != cudaSuccess) break;
     if ((ce = cudaStreamWaitEvent(ctx->s_out, ev[2 * c + 1], 0)) != cudaSuccess) break;
     rc = out(s0, m, ctx->s_out);
   }
-  // Every stream settles before the events go and before an error returns.
+  // The context's stream takes the second lane's work back, and every stream
+  // settles before the events go and before an error returns.
+  if (cudaEventRecord(ev[2 * k + 1], lane->stream) == cudaSuccess) cudaStreamWaitEvent(ctx->stream, ev[2 * k + 1], 0);
   cudaStreamSynchronize(ctx->s_in);
+  cudaStreamSynchronize(lane->stream);
   cudaStreamSynchronize(ctx->stream);
   const cudaError_t se = cudaStreamSynchronize(ctx->s_out);
   for (auto& e : ev) cudaEventDestroy(e);
-  if (rc) return rc;
+  ctx->launches += lane->launches - lane_launches;
+  if (rc) return failed == ctx ? rc : fail(ctx, rc, lane->err.c_str());
   if (ce != cudaSuccess) return cuda_fail(ctx, "chunked host-buffer call", ce);
   if (se != cudaSuccess) return cuda_fail(ctx, "chunked host-buffer call", se);
   return SQ_OK;

@@ -51,6 +51,7 @@ struct sq_ctx {
   float window = 0x1p-16f;        // relative window past the limit within which near-first still visits nodes
   int layout = SQ_LAYOUT_BINARY;  // node records of near-first nearest rays (SQ_LAYOUT_*)
   cudaStream_t s_in = nullptr, s_out = nullptr;  // copy streams of the chunked host-buffer calls (made on first use)
+  sq_ctx* lane = nullptr;  // second compute lane of the chunked host-buffer calls (own stream and scratch; made on first use)
   uint64_t launches = 0;
   std::unordered_map<uint64_t, int> occ;  // (kernel, dynamic smem) -> resident blocks per SM
 };
@@ -109,14 +110,18 @@ constexpr uint32_t kMaxCustomStride = 32;
 int32_t rtc_kernel_set(uint32_t stride, const char* src, KernelSet* out, std::string* log);
 
 // Host-buffer calls in chunks: chunk c's inputs are copied in on the
-// context's copy-in stream while chunk c - 1 runs on the context's stream,
-// whose results are copied out on the copy-out stream meanwhile (sq_api.cu).
+// context's copy-in stream while earlier chunks run, and their results are
+// copied out on the copy-out stream meanwhile (sq_api.cu). Chunks alternate
+// between two compute lanes, the context itself and ctx->lane (its own
+// stream, launch counters and replay list), so that one chunk's first
+// launches fill the SMs left idle by the other's last long queries.
 // in(s, m, stream) / out(s, m, stream) enqueue the copies of queries
-// [s, s + m); run(s, m) enqueues the work on ctx->stream. One chunk when n is
-// small. Returns when every copy out has landed.
+// [s, s + m); run(lane, s, m) enqueues the work on lane->stream using only
+// that lane's scratch. One chunk when n is small. Returns when every copy out
+// has landed.
 uint32_t pipeline_chunks(uint32_t n);
 int32_t pipelined(sq_ctx* ctx, uint32_t n, const std::function<int32_t(uint32_t, uint32_t, cudaStream_t)>& in,
-                  const std::function<int32_t(uint32_t, uint32_t)>& run,
+                  const std::function<int32_t(sq_ctx*, uint32_t, uint32_t)>& run,
                   const std::function<int32_t(uint32_t, uint32_t, cudaStream_t)>& out);
 
 // Sorts each CSR segment [offsets[i], offsets[i+1]) of `leaves` ascending

@@ -1,8 +1,10 @@
 """Host-buffer calls large enough to run in chunks (rays copied in on one
-stream while earlier chunks are walked and their hits copied out on
-another) return exactly what the device-pointer calls and the oracle
-return: plain nearest with every output and per-ray limits, and the
-learned-seeded call."""
+stream while earlier chunks are walked, alternately on the context's stream
+and on its second lane, and their hits copied out on another) return exactly
+what the device-pointer calls and the oracle return: plain nearest with every
+output and per-ray limits, in both traversal orders and both node layouts
+(the second lane takes the context's settings), and the learned-seeded
+call."""
 import numpy as np
 import pytest
 
@@ -36,6 +38,22 @@ def test_chunked_plain_equals_oracle(setup):
     ref = o.nearest(rays, mt)
     assert (ref.leaf != O.NO_HIT).mean() > 0.3
     assert_same_nearest(ref, got, label="chunked host call")
+
+
+@pytest.mark.parametrize("order,layout", [(sq.ORDER_REFERENCE, sq.LAYOUT_BINARY), (sq.ORDER_NEAR_FIRST, sq.LAYOUT_WIDE)])
+def test_chunked_settings_reach_both_lanes(setup, order, layout):
+    s, rays, ctx, geom, scene = setup
+    ctx.set_order(order)
+    ctx.set_layout(layout)
+    try:
+        launches0 = ctx.launch_count
+        got = scene.raycast_nearest(rays, s["max_toi"], outputs=("normal",))
+        assert ctx.launch_count - launches0 >= 4  # every chunk's launches are counted, both lanes'
+    finally:
+        ctx.set_order(sq.ORDER_NEAR_FIRST)
+        ctx.set_layout(sq.LAYOUT_BINARY)
+    ref = O.Scene("tris", 3, s["prims"]).nearest(rays, s["max_toi"])
+    assert_same_nearest(ref, got, label=f"chunked host call, order {order}, layout {layout}")
 
 
 def test_chunked_guided_equals_device_call(setup):
