@@ -68,6 +68,29 @@ def parse():
     return ap.parse_args()
 
 
+def rank_rays(s, rank):
+    """Weak scaling: rank 0 walks the workload's own rays; every other rank
+    its own batch of the same two kinds and size (seed 1 + 1000 * rank). The
+    scene is replicated; no rank reads another's rays or hits."""
+    if rank == 0:
+        return s["rays"]
+    nx, ny = s["grid"]
+    n = s["rays"].shape[0]
+    from spatial_query_b200 import scenes
+    return scenes.terrain_rays(scenes.Rng(1 + 1000 * rank), nx, ny, *s["zrange"], n // 2, n - n // 2)
+
+
+def max_over_ranks(x, dist=None, device=None):
+    """The largest x over all ranks (the job's step time is its slowest
+    rank's); x itself with one process."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -541,10 +564,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     s = scenes.terrain_scene(seed=1)
-    if rank > 0:
-        # Weak scaling: each rank its own ray batch of the same two kinds.
-        nx, ny = s["grid"]
-        s["rays"] = scenes.terrain_rays(scenes.Rng(1 + 1000 * rank), nx, ny, *s["zrange"], nx * ny, nx * ny)
+    s["rays"] = rank_rays(s, rank)
     if args.rays != s["rays"].shape[0]:
         half, total = args.rays // 2, s["rays"].shape[0]
         s["rays"] = np.ascontiguousarray(np.concatenate([s["rays"][:half], s["rays"][total // 2: total // 2 + half]]))
@@ -667,12 +687,7 @@ def main():
     torch.cuda.synchronize()
 
     def mean_max(xs):
-        m = sum(xs) / len(xs)
-        if dist:
-            t = torch.tensor([m], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            m = float(t.item())
-        return m
+        return max_over_ranks(sum(xs) / len(xs), dist, dev)
 
     # Config 2's second query: all hits, the first 16 per ray in order, plus full counts.
     K_ALL = 16
