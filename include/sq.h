@@ -21,8 +21,15 @@
  *            same (toi, leaf) total order (query/hit.rs:77-84).
  *
  * Host-buffer entry points copy inputs in and results out on the context's
- * stream and return when the results are in host memory. The `_d` variants
- * take device pointers, enqueue on the context's stream and return at once.
+ * stream and return when the results are in host memory. Nearest calls of
+ * 524,288 queries or more (sq_raycast_nearest, sq_shapecast_nearest,
+ * sq_raycast_nearest_guided) without stats run in two or four chunks: rays
+ * copied in and hits copied out on two internal copy streams while chunks
+ * are walked, alternately on the context's stream and on a second internal
+ * context (its own stream and scratch, same settings); all of them have
+ * settled when the call returns. Host buffers in page-locked memory let the
+ * copies overlap. The `_d` variants take device pointers, enqueue on the
+ * context's stream and return at once.
  *
  * Threading: a context is used by one host thread at a time; uploaded scenes
  * may be shared by contexts on the same device.
