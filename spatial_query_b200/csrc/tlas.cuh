@@ -304,10 +304,11 @@ template <int D> struct TLane {
 
 // The mesh-instance walk (the two-level benchmark's kernel) is latency-bound
 // with divergent lanes, so resident warps count more than registers: it is
-// held to six resident blocks per SM (80 registers, a few spilled), which
-// measured 7.1 ms per million rays against 8.8 ms at its natural 112.
+// held to five resident blocks per SM (96 registers, a few spilled), which
+// measured 3.87 ms per two-level frame against 4.29 ms at six blocks (80
+// registers) and 3.89 ms at four.
 template <int D, int IK, bool REF, bool STATS>
-__global__ void __launch_bounds__(kThreads, (IK == kInstMesh && !REF && !STATS) ? 6 : 1)
+__global__ void __launch_bounds__(kThreads, (IK == kInstMesh && !REF && !STATS) ? 5 : 1)
     tlas_kernel(const TlasParams p) {
   using IL = InstLayout<D, IK>;
   using NL = NodeLayout<D>;
@@ -646,6 +647,149 @@ __global__ void __launch_bounds__(kThreads, (IK == kInstMesh && !REF && !STATS) 
     }
   };
 
+  // Mesh instances, nearest rays: a lane walks its instances' BLASes inside
+  // the same descent loop as the top level, one leaf per pass, so that lanes
+  // in different levels and instances share the node-test instructions
+  // instead of each lane finishing a whole BLAS walk (blas_nearest) while
+  // the rest of its warp waits. Same visits, same order, same answers.
+  bool in_blas = false;
+  bool b_last = false;    // the instance is the last of its top-level leaf
+  uint32_t b_pos = 0;     // instance record whose BLAS is walked
+  int b_base = 0;         // stack depth at BLAS entry
+  RayPre<3> b_r;          // the ray in instance space (origin divided by the scale)
+  bool b_fast = false;
+  float b_limit = 0.f, b_cut = 0.f, b_t = 0.f;
+  uint32_t b_best = kNoHit, b_flag = 0u;
+  float b_n[3] = {0.f, 0.f, 0.f};
+  auto unified = [&]() { return IK == kInstMesh && L.kind == kTRayNearest; };
+
+  // blas_nearest's box test and leaf, on the lane's BLAS state.
+  auto btest = [&](const float* lo, const float* hi, float& te) -> bool {
+    int ax;
+    const bool geo = b_fast ? slab_fast<3>(b_r, lo, hi, kInf, te) : slab<3>(b_r, lo, hi, kInf, te, ax);
+    return geo && te <= b_cut;
+  };
+  auto blas_leaf = [&]() {
+    uint32_t pos = L.code & ~kLeafBit;
+    for (;;) {
+      float rec[12];
+      load_vec<3>(p.bprims + size_t(pos) * 3, rec);
+      const uint32_t idw = __float_as_uint(rec[9]);
+      const uint32_t id = idw & ~kLeafBit;
+      float t, nrm[3];
+      if (ray_triangle(b_r.o, b_r.d, rec, rec + 3, rec + 6, t) && !(t > b_limit)) {
+        if (b_best == kNoHit || hit_before(t, id, b_t, b_best)) {
+          tri_normal(rec, rec + 3, rec + 6, nrm);
+          b_best = id;
+          b_t = t;
+          b_limit = t;
+          b_cut = t;
+          if (!REF && !L.ref) {
+            // certify the new best: not before its own triangle's AABB entry
+            float lo[3], hi[3], te;
+            int ax;
+            tri_aabb(rec, rec + 3, rec + 6, lo, hi);
+            if (b_fast) slab_fast<3>(b_r, lo, hi, kInf, te);
+            else slab<3>(b_r, lo, hi, kInf, te, ax);
+            b_flag = uint32_t(t < te);
+            b_cut = near_limit(t, p.window);
+          }
+          b_n[0] = nrm[0];
+          b_n[1] = nrm[1];
+          b_n[2] = nrm[2];
+        }
+      }
+      if (idw & kLeafBit) break;
+      ++pos;
+    }
+  };
+  // Pops within the lane's current level: the BLAS's own entries when in
+  // one (false: the BLAS is exhausted), else the top level's (pop).
+  auto pop_level = [&]() -> bool {
+    if (in_blas) {
+      while (L.sp > b_base) {
+        --L.sp;
+        L.code = s_code[L.sp * kThreads + tid];
+        const float t = s_t[L.sp * kThreads + tid];
+        if (t <= b_cut) return true;
+      }
+      return false;
+    }
+    return pop();
+  };
+  // The instances of a top-level leaf from record `pos` on, as leaf() takes
+  // them for a nearest ray: the first accepted one whose BLAS root the
+  // instance-space ray enters starts its walk (true); false when the leaf
+  // has no such instance left.
+  auto enter_from = [&](uint32_t pos) -> bool {
+    if constexpr (IK == kInstMesh) {
+      for (;;) {
+        float rec[IL::vec * 4];
+        load_vec<IL::vec>(p.insts + size_t(pos) * IL::vec, rec);
+        const uint32_t idw = __float_as_uint(rec[IL::id]);
+        const uint32_t id = idw & ~kLeafBit;
+        if (t_accepts(p, id)) {
+          if (STATS) L.v_nar += 1;
+          // World ray -> instance space (tlas.rs:465-471).
+          const float* R = rec + IL::rot;
+          const float* tr = rec + IL::trans;
+          float v[3], lo[3], ld[3];
+#pragma unroll
+          for (int i = 0; i < 3; ++i) v[i] = fsub(L.r.o[i], tr[i]);
+          rotate_t<3>(R, v, lo);
+          rotate_t<3>(R, L.r.d, ld);
+          const float sc = rec[IL::param];
+#pragma unroll
+          for (int i = 0; i < 3; ++i) {
+            b_r.o[i] = fdiv(lo[i], sc);
+            b_r.d[i] = ld[i];
+          }
+          ray_prep<3>(b_r);
+          bool f = p.blas_finite && b_r.par == 0u && isfinite(sc);
+#pragma unroll
+          for (int i = 0; i < 3; ++i) f = f && isfinite(b_r.o[i]) && isfinite(b_r.d[i]);
+          const float mts = fdiv(L.limit, sc);
+          b_fast = f && !isnan(mts);
+          b_limit = mts;
+          b_cut = mts;
+          const BlasRoot br = p.broots[__float_as_uint(rec[IL::blas])];
+          float te;
+          if (btest(br.lo, br.hi, te)) {
+            in_blas = true;
+            b_last = (idw & kLeafBit) != 0u;
+            b_pos = pos;
+            b_base = L.sp;
+            b_best = kNoHit;
+            b_flag = 0u;
+            b_t = 0.f;
+            L.code = br.code;
+            return true;
+          }
+        }
+        if (idw & kLeafBit) return false;
+        ++pos;
+      }
+    }
+    return false;
+  };
+  // The BLAS is exhausted: its nearest hit, scaled and rotated back to
+  // world space, is the instance's hit (as after blas_nearest in leaf()).
+  auto blas_finish = [&]() {
+    in_blas = false;
+    if constexpr (IK == kInstMesh) {
+      if (b_best == kNoHit) return;
+      float rec[IL::vec * 4];
+      load_vec<IL::vec>(p.insts + size_t(b_pos) * IL::vec, rec);
+      const float toi = fmul(b_t, rec[IL::param]);
+      if (!(toi > L.limit)) {
+        float nw[3];
+        rotate<3>(rec + IL::rot, b_n, nw);
+        if (STATS) L.v_hit += 1;
+        take(toi, __float_as_uint(rec[IL::id]) & ~kLeafBit, b_best, nw, b_pos, b_flag);
+      }
+    }
+  };
+
   bool pending = false;  // this lane's query waits to be answered again in reference order
   uint32_t pending_g = 0;
   for (;;) {
@@ -671,6 +815,7 @@ __global__ void __launch_bounds__(kThreads, (IK == kInstMesh && !REF && !STATS) 
     }
     if (gs != kNoHit) {
       L.ref = replay;
+      in_blas = false;
       live = start(gs);
       if (!live) finish();
     }
@@ -680,15 +825,23 @@ __global__ void __launch_bounds__(kThreads, (IK == kInstMesh && !REF && !STATS) 
     }
     if (live) {
       bool done = false;
+      // Descend interior records until a leaf comes up: the top level's, or
+      // the BLAS's for a lane inside an instance (the same record layout).
       while (!(L.code & kLeafBit)) {
         float rec[NL::vec * 4];
-        load_vec<NL::vec>(p.nodes + size_t(L.code) * NL::vec, rec);
+        load_vec<NL::vec>((in_blas ? p.bnodes : p.nodes) + size_t(L.code) * NL::vec, rec);
         const uint32_t ca = __float_as_uint(rec[4 * D]);
         const uint32_t cb = __float_as_uint(rec[4 * D + 1]);
         float ta, tb;
-        const bool pa = test_box(rec, rec + D, ta);
-        const bool pb = test_box(rec + 2 * D, rec + 3 * D, tb);
-        if (STATS) L.v_nodes += 2;
+        bool pa, pb;
+        if (IK == kInstMesh && in_blas) {
+          pa = btest(rec, rec + 3, ta);
+          pb = btest(rec + 6, rec + 9, tb);
+        } else {
+          pa = test_box(rec, rec + D, ta);
+          pb = test_box(rec + 2 * D, rec + 3 * D, tb);
+          if (STATS) L.v_nodes += 2;
+        }
         if (pa && pb) {
           const bool a_first = (REF || !is_nearest()) ? false : (!L.ref && ta <= tb);
           s_code[L.sp * kThreads + tid] = a_first ? cb : ca;
@@ -699,12 +852,29 @@ __global__ void __launch_bounds__(kThreads, (IK == kInstMesh && !REF && !STATS) 
           L.code = ca;
         } else if (pb) {
           L.code = cb;
-        } else if (!pop()) {
+        } else if (!pop_level()) {
           done = true;
           break;
         }
       }
-      if (!done) {
+      if (unified()) {
+        if (in_blas) {
+          // `done` here: the BLAS is exhausted, not the query.
+          if (!done) {
+            blas_leaf();
+            done = !pop_level();
+          }
+          if (done) {
+            const bool last = b_last;
+            const uint32_t next = b_pos + 1;
+            blas_finish();
+            done = false;
+            if (last || !enter_from(next)) done = !pop();
+          }
+        } else if (!done && !enter_from(L.code & ~kLeafBit)) {
+          done = !pop();
+        }
+      } else if (!done) {
         leaf();
         done = !pop();
       }
