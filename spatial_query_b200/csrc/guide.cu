@@ -1198,6 +1198,51 @@ extern "C" int32_t sq_raycast_nearest_guided_d(sq_ctx* ctx, const sq_bvh* b, con
   if (g->bvh != b) return fail(ctx, SQ_ERR_INVALID, "the guide was built for another scene");
   int32_t rc;
   const int32_t* seeds = d_bucket;
+  if (!seeds && !stats && n >= (1u << 19)) {
+    // Two halves, one on the context's stream and one on its second lane:
+    // the second half's inference fills the SMs that the first half's
+    // traversal tail leaves idle. Seeds and hits land where one launch
+    // would put them.
+    if ((rc = arena_reserve(ctx, size_t(n) * 4))) return rc;
+    int32_t* d = static_cast<int32_t*>(ctx->arena.p);
+    sq_ctx* lane = nullptr;
+    if ((rc = sqi::second_lane(ctx, &lane))) return rc;
+    sq_ctx* saved = g->ctx;
+    g->ctx = ctx;
+    rc = refresh_images(g);  // once, before either half predicts
+    g->ctx = saved;
+    if (rc) return rc;
+    const uint64_t lane_launches = lane->launches;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    for (auto& e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaError_t ce = cudaEventRecord(ev[0], ctx->stream);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(lane->stream, ev[0], 0);
+    const uint32_t m0 = (n / 2 + 255) / 256 * 256;
+    sq_ctx* failed = nullptr;
+    for (int k = 0; k < 2 && ce == cudaSuccess && !failed; ++k) {
+      sq_ctx* on = k ? lane : ctx;
+      const uint32_t s0 = k ? m0 : 0, m = k ? n - m0 : m0;
+      sq_hits c = *out;
+      c.leaf += s0;
+      if (c.toi) c.toi += s0;
+      if (c.sub_object) c.sub_object += s0;
+      if (c.normal) c.normal += size_t(s0) * 3;
+      if (c.point) c.point += size_t(s0) * 3;
+      g->ctx = on;
+      rc = predict(g, d_rays + size_t(s0) * 6, m, d + s0);
+      g->ctx = saved;
+      if (!rc) rc = seeded_nearest(on, b, d_rays + size_t(s0) * 6, m, max_toi, d + s0, g->d_buckets, g->n_buckets, c,
+                                   nullptr);
+      if (rc) failed = on;
+    }
+    // The context's stream takes the lane's half back in every case.
+    if (cudaEventRecord(ev[1], lane->stream) == cudaSuccess) cudaStreamWaitEvent(ctx->stream, ev[1], 0);
+    for (auto& e : ev) cudaEventDestroy(e);
+    ctx->launches += lane->launches - lane_launches;
+    if (failed) return failed == ctx ? rc : fail(ctx, rc, lane->err.c_str());
+    if (ce != cudaSuccess) return cuda_fail(ctx, "guided halves", ce);
+    return SQ_OK;
+  }
   if (!seeds && n) {
     if ((rc = arena_reserve(ctx, size_t(n) * 4))) return rc;
     int32_t* d = static_cast<int32_t*>(ctx->arena.p);

@@ -1201,6 +1201,22 @@ int32_t sqi::sort_csr_segments(sq_ctx* ctx, uint32_t* d_leaves, uint64_t total, 
   return SQ_OK;
 }
 
+int32_t sqi::second_lane(sq_ctx* ctx, sq_ctx** out) {
+  if (!ctx->lane) {
+    sq_ctx* l = nullptr;
+    int32_t rc = sq_ctx_create(ctx->device, &l);
+    if (rc) return fail(ctx, rc, "second compute lane");
+    ctx->lane = l;
+  }
+  sq_ctx* lane = ctx->lane;
+  lane->order = ctx->order;
+  lane->blocks_per_sm = ctx->blocks_per_sm;
+  lane->window = ctx->window;
+  lane->layout = ctx->layout;
+  *out = lane;
+  return SQ_OK;
+}
+
 uint32_t sqi::pipeline_chunks(uint32_t n) {
   // Chunks of at least 262,144 queries: below that the launch tails cost
   // more than the copies they hide.
@@ -1221,16 +1237,8 @@ int32_t sqi::pipelined(sq_ctx* ctx, uint32_t n, const std::function<int32_t(uint
   }
   if (!ctx->s_in) CK(cudaStreamCreateWithFlags(&ctx->s_in, cudaStreamNonBlocking));
   if (!ctx->s_out) CK(cudaStreamCreateWithFlags(&ctx->s_out, cudaStreamNonBlocking));
-  if (!ctx->lane) {
-    sq_ctx* l = nullptr;
-    if ((rc = sq_ctx_create(ctx->device, &l))) return fail(ctx, rc, "second compute lane");
-    ctx->lane = l;
-  }
-  sq_ctx* lane = ctx->lane;
-  lane->order = ctx->order;
-  lane->blocks_per_sm = ctx->blocks_per_sm;
-  lane->window = ctx->window;
-  lane->layout = ctx->layout;
+  sq_ctx* lane = nullptr;
+  if ((rc = second_lane(ctx, &lane))) return rc;
   const uint64_t lane_launches = lane->launches;
   std::vector<cudaEvent_t> ev(2 * k + 2, nullptr);
   for (auto& e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
