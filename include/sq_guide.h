@@ -91,7 +91,12 @@ int32_t sq_guide_predict_d(sq_guide* g, const float* d_rays, uint32_t n, int32_t
 
 /* Learned-seeded nearest rays (device pointers): same outputs, same hits as
  * sq_raycast_nearest_d. `d_bucket` NULL runs the network first (into the
- * context's arena); otherwise the given predictions seed the queries. */
+ * context's arena); otherwise the given predictions seed the queries. With
+ * `d_bucket` NULL, no stats and 524,288 rays or more, the two halves are
+ * predicted and walked on the context's stream and on its internal second
+ * lane (own stream and scratch, joined back to the context's stream before
+ * the call returns); the first such call of a batch size sizes that lane's
+ * scratch, so it belongs outside a stream capture. */
 int32_t sq_raycast_nearest_guided_d(sq_ctx* ctx, const sq_bvh* bvh, const sq_guide* g, const float* d_rays,
                                     uint32_t n, float max_toi, const int32_t* d_bucket, const sq_hits* out,
                                     sq_query_stats* stats);
