@@ -8,14 +8,18 @@
 // coordinate under f32::total_cmp and split at start + count / 2.
 //
 // How: the recursion runs a level at a time. For every segment of a level
-// (a node's range of the primitive order), one group of threads reduces the
-// node's box and its centroid box, decides leaf or split, and writes the sort
-// key of each of its primitives; one segmented stable sort then orders every
-// split segment of the level at once, which is the per-node stable sort of
-// the crate (ties keep the order the parent's sort left). Nodes are numbered
-// in level order as they are made; preorder numbers follow from subtree sizes
+// (a node's range of the primitive order) the node's box and its centroid
+// box are reduced (one warp per segment on the wide levels; many blocks per
+// segment with order-preserving integer atomics on the top levels, whose
+// few segments are long), leaf or split is decided, and each primitive of a
+// split segment gets the sort key (segment start << 32 | its split-axis key);
+// every other position keeps (position << 32). One stable radix sort of the
+// level on those keys then orders every split segment in place, which is the
+// per-node stable sort of the crate (ties keep the order the parent's sort
+// left), and leaves every other position where it is. Nodes are numbered in
+// level order as they are made; preorder numbers follow from subtree sizes
 // (bottom-up, a level at a time) and left-subtree offsets (top-down).
-#include <cub/device/device_segmented_sort.cuh>
+#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <vector>
@@ -68,22 +72,159 @@ struct LevelParams {
   const Seg* cur;
   uint32_t m;            // segments of this level
   Seg* next;             // the next level's segments (appended)
-  uint32_t* counters;    // [0] next segments, [1] nodes made, [2] sort segments
+  uint32_t* counters;    // [0] next segments, [1] nodes made, [2] split segments
   LNode* nodes;          // by level-order id
   float* bounds;         // by level-order id: min[D], max[D]
-  uint32_t* sort_beg;
-  uint32_t* sort_end;
-  uint32_t* sort_keys;   // per position: the key of its segment's split axis
+  unsigned long long* sort_keys;  // per position: (segment start << 32) | split-axis key, or (position << 32)
+  uint32_t* red;         // top levels: per segment 4 x kMaxDim ordered bounds (box lo, hi, centroid lo, hi)
+  int* axis;             // top levels: per segment the split axis, -1 for a leaf
+  uint32_t chunk;        // top levels: positions per block
 };
 
-// One group of TPS threads per segment (TPS = 32: a warp; TPS = blockDim:
-// the whole block, for the few large segments of the top levels).
+// f32 <-> an unsigned key with the same order (total_ukey), for min / max
+// by integer atomics; NaN coordinates are skipped, as fminf / fmaxf skip them.
+__device__ __forceinline__ float ukey_float(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+
+// Leaf or split of segment sg from its reduced boxes (tree.rs:129-154):
+// writes the node's bounds and record, appends the children's segments,
+// and returns the split axis (-1: leaf). One thread per segment.
+__device__ int decide(const LevelParams& p, const Seg& sg, const float* lo, const float* hi, const float* clo,
+                      const float* chi) {
+  const int D = p.D;
+  const uint32_t count = sg.e - sg.s;
+  float* bo = p.bounds + size_t(sg.node) * 2 * D;
+  for (int k = 0; k < D; ++k) {
+    bo[k] = lo[k];
+    bo[D + k] = hi[k];
+  }
+  LNode nd{sg.s, sg.e, kNone, kNone};
+  int axis = -1;
+  if (count > kLeafSize) {
+    int ax = 0;
+    float ext[kMaxDim];
+    for (int k = 0; k < D; ++k) ext[k] = __fsub_rn(chi[k], clo[k]);
+    for (int k = 1; k < D; ++k)
+      if (ext[k] > ext[ax]) ax = k;
+    if (ext[ax] > kEps) {
+      axis = ax;
+      const uint32_t mid = sg.s + count / 2;
+      const uint32_t c0 = atomicAdd(&p.counters[0], 2u);
+      const uint32_t id0 = atomicAdd(&p.counters[1], 2u);
+      p.next[c0] = Seg{sg.s, mid, id0};
+      p.next[c0 + 1] = Seg{mid, sg.e, id0 + 1};
+      nd.a = id0;
+      nd.b = id0 + 1;
+      atomicAdd(&p.counters[2], 1u);
+    }
+  }
+  p.nodes[sg.node] = nd;
+  return axis;
+}
+
+// Every position keeps its place unless a split segment claims it.
+__global__ void place_keys_kernel(unsigned long long* sort_keys, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    sort_keys[i] = (unsigned long long)i << 32;
+}
+
+// Top levels: empty per-segment bounds (+inf for the minima, -inf for the maxima).
+__global__ void red_init_kernel(uint32_t* red, uint32_t m) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m * 4 * kMaxDim) return;
+  const uint32_t part = (i / kMaxDim) % 4;  // 0 lo, 1 hi, 2 centroid lo, 3 centroid hi
+  red[i] = (part == 0 || part == 2) ? total_ukey(INFINITY) : total_ukey(-INFINITY);
+}
+
+// Top levels: block (c, g) reduces positions [s + c * chunk, s + (c + 1) * chunk)
+// of segment g and folds its result into the segment's bounds.
+__global__ void __launch_bounds__(256) red_kernel(const LevelParams p) {
+  const uint32_t g = blockIdx.y;
+  const Seg sg = p.cur[g];
+  const uint64_t b0 = uint64_t(sg.s) + uint64_t(blockIdx.x) * p.chunk;
+  if (b0 >= sg.e) return;  // uniform per block
+  const uint32_t b1 = uint32_t(std::min<uint64_t>(sg.e, b0 + p.chunk));
+  const int D = p.D;
+  float lo[kMaxDim], hi[kMaxDim], clo[kMaxDim], chi[kMaxDim];
+#pragma unroll
+  for (int k = 0; k < kMaxDim; ++k) {
+    lo[k] = clo[k] = INFINITY;
+    hi[k] = chi[k] = -INFINITY;
+  }
+  for (uint32_t pos = uint32_t(b0) + threadIdx.x; pos < b1; pos += blockDim.x) {
+    const float* b = p.aabbs + size_t(p.idx[pos]) * 2 * D;
+#pragma unroll
+    for (int k = 0; k < kMaxDim; ++k) {
+      if (k < D) {
+        lo[k] = fminf(lo[k], b[k]);
+        hi[k] = fmaxf(hi[k], b[D + k]);
+        const float c = centre(b, D, k);
+        clo[k] = fminf(clo[k], c);
+        chi[k] = fmaxf(chi[k], c);
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int k = 0; k < kMaxDim; ++k) {
+      if (k < D) {
+        lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+        hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+        clo[k] = fminf(clo[k], __shfl_xor_sync(0xffffffffu, clo[k], o));
+        chi[k] = fmaxf(chi[k], __shfl_xor_sync(0xffffffffu, chi[k], o));
+      }
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    uint32_t* r = p.red + size_t(g) * 4 * kMaxDim;
+    for (int k = 0; k < D; ++k) {
+      if (!isnan(lo[k])) atomicMin(&r[k], total_ukey(lo[k]));
+      if (!isnan(hi[k])) atomicMax(&r[kMaxDim + k], total_ukey(hi[k]));
+      if (!isnan(clo[k])) atomicMin(&r[2 * kMaxDim + k], total_ukey(clo[k]));
+      if (!isnan(chi[k])) atomicMax(&r[3 * kMaxDim + k], total_ukey(chi[k]));
+    }
+  }
+}
+
+// Top levels: leaf or split per segment from the reduced bounds.
+__global__ void decide_kernel(const LevelParams p) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= p.m) return;
+  const uint32_t* r = p.red + size_t(g) * 4 * kMaxDim;
+  float lo[kMaxDim], hi[kMaxDim], clo[kMaxDim], chi[kMaxDim];
+  for (int k = 0; k < p.D; ++k) {
+    lo[k] = ukey_float(r[k]);
+    hi[k] = ukey_float(r[kMaxDim + k]);
+    clo[k] = ukey_float(r[2 * kMaxDim + k]);
+    chi[k] = ukey_float(r[3 * kMaxDim + k]);
+  }
+  p.axis[g] = decide(p, p.cur[g], lo, hi, clo, chi);
+}
+
+// Top levels: the sort keys of the split segments' positions, chunked like red_kernel.
+__global__ void split_keys_kernel(const LevelParams p) {
+  const uint32_t g = blockIdx.y;
+  const int axis = p.axis[g];
+  if (axis < 0) return;
+  const Seg sg = p.cur[g];
+  const uint64_t b0 = uint64_t(sg.s) + uint64_t(blockIdx.x) * p.chunk;
+  if (b0 >= sg.e) return;
+  const uint32_t b1 = uint32_t(std::min<uint64_t>(sg.e, b0 + p.chunk));
+  const uint32_t* key = p.keys + size_t(axis) * p.n;
+  for (uint32_t pos = uint32_t(b0) + threadIdx.x; pos < b1; pos += blockDim.x)
+    p.sort_keys[pos] = ((unsigned long long)sg.s << 32) | key[p.idx[pos]];
+}
+
+// Wide levels: one warp per segment.
 template <int TPS>
 __global__ void __launch_bounds__(256) level_kernel(const LevelParams p) {
+  static_assert(TPS == 32, "one warp per segment");
   const uint32_t groups = blockDim.x / TPS;
   const uint32_t g = blockIdx.x * groups + threadIdx.x / TPS;
   const uint32_t lane = threadIdx.x % TPS;
-  if (g >= p.m) return;  // uniform per group (and per block when TPS == blockDim)
+  if (g >= p.m) return;  // uniform per warp
   const int D = p.D;
   const Seg sg = p.cur[g];
   float lo[kMaxDim], hi[kMaxDim], clo[kMaxDim], chi[kMaxDim];
@@ -118,72 +259,14 @@ __global__ void __launch_bounds__(256) level_kernel(const LevelParams p) {
       }
     }
   }
-  __shared__ float red[8][4 * kMaxDim];
-  __shared__ int s_axis;
-  if constexpr (TPS > 32) {
-    const uint32_t w = threadIdx.x / 32;
-    if ((threadIdx.x & 31) == 0) {
-      for (int k = 0; k < D; ++k) {
-        red[w][k] = lo[k];
-        red[w][kMaxDim + k] = hi[k];
-        red[w][2 * kMaxDim + k] = clo[k];
-        red[w][3 * kMaxDim + k] = chi[k];
-      }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (uint32_t v = 1; v < TPS / 32; ++v) {
-        for (int k = 0; k < D; ++k) {
-          lo[k] = fminf(lo[k], red[v][k]);
-          hi[k] = fmaxf(hi[k], red[v][kMaxDim + k]);
-          clo[k] = fminf(clo[k], red[v][2 * kMaxDim + k]);
-          chi[k] = fmaxf(chi[k], red[v][3 * kMaxDim + k]);
-        }
-      }
-    }
-  }
-  // Leaf or split (tree.rs:129-154), decided by the group's first thread.
+  // Leaf or split, decided by the warp's first lane.
   int axis = -1;
-  if (lane == 0) {
-    const uint32_t count = sg.e - sg.s;
-    float* bo = p.bounds + size_t(sg.node) * 2 * D;
-    for (int k = 0; k < D; ++k) {
-      bo[k] = lo[k];
-      bo[D + k] = hi[k];
-    }
-    LNode nd{sg.s, sg.e, kNone, kNone};
-    if (count > kLeafSize) {
-      int ax = 0;
-      float ext[kMaxDim];
-      for (int k = 0; k < D; ++k) ext[k] = __fsub_rn(chi[k], clo[k]);
-      for (int k = 1; k < D; ++k)
-        if (ext[k] > ext[ax]) ax = k;
-      if (ext[ax] > kEps) {
-        axis = ax;
-        const uint32_t mid = sg.s + count / 2;
-        const uint32_t c0 = atomicAdd(&p.counters[0], 2u);
-        const uint32_t id0 = atomicAdd(&p.counters[1], 2u);
-        p.next[c0] = Seg{sg.s, mid, id0};
-        p.next[c0 + 1] = Seg{mid, sg.e, id0 + 1};
-        nd.a = id0;
-        nd.b = id0 + 1;
-        const uint32_t q = atomicAdd(&p.counters[2], 1u);
-        p.sort_beg[q] = sg.s;
-        p.sort_end[q] = sg.e;
-      }
-    }
-    p.nodes[sg.node] = nd;
-  }
-  if constexpr (TPS > 32) {
-    if (threadIdx.x == 0) s_axis = axis;
-    __syncthreads();
-    axis = s_axis;
-  } else {
-    axis = __shfl_sync(0xffffffffu, axis, 0);
-  }
+  if (lane == 0) axis = decide(p, sg, lo, hi, clo, chi);
+  axis = __shfl_sync(0xffffffffu, axis, 0);
   if (axis < 0) return;
   const uint32_t* key = p.keys + size_t(axis) * p.n;
-  for (uint32_t pos = sg.s + lane; pos < sg.e; pos += TPS) p.sort_keys[pos] = key[p.idx[pos]];
+  for (uint32_t pos = sg.s + lane; pos < sg.e; pos += TPS)
+    p.sort_keys[pos] = ((unsigned long long)sg.s << 32) | key[p.idx[pos]];
 }
 
 // Subtree node counts, one level at a time from the deepest.
@@ -251,22 +334,24 @@ extern "C" int32_t sq_tree_build_d(sq_ctx* ctx, int32_t dim, uint32_t n, const f
 
   // Scratch, carved from one stream-ordered allocation.
   sqi::Carve cv;
+  constexpr uint32_t kWide = 1024;  // levels with this many segments or more: one warp per segment
   const size_t o_keys = cv.take(size_t(D) * n * 4), o_idx0 = cv.take(size_t(n) * 4), o_idx1 = cv.take(size_t(n) * 4),
-               o_sk0 = cv.take(size_t(n) * 4), o_sk1 = cv.take(size_t(n) * 4),
+               o_sk0 = cv.take(size_t(n) * 8), o_sk1 = cv.take(size_t(n) * 8),
                o_seg0 = cv.take((size_t(n) + 1) * sizeof(Seg)), o_seg1 = cv.take((size_t(n) + 1) * sizeof(Seg)),
-               o_beg = cv.take(size_t(n) * 4), o_end = cv.take(size_t(n) * 4), o_nodes = cv.take(N2 * sizeof(LNode)),
-               o_lb = cv.take(N2 * 2 * D * 4), o_size = cv.take(N2 * 4), o_pre = cv.take(N2 * 4), o_ctr = cv.take(16);
+               o_red = cv.take(size_t(kWide) * 4 * kMaxDim * 4), o_axis = cv.take(size_t(kWide) * 4),
+               o_nodes = cv.take(N2 * sizeof(LNode)), o_lb = cv.take(N2 * 2 * D * 4), o_size = cv.take(N2 * 4),
+               o_pre = cv.take(N2 * 4), o_ctr = cv.take(16);
   char* base = nullptr;
   CK(cudaMallocAsync(reinterpret_cast<void**>(&base), cv.off, st));
   uint32_t* keys = reinterpret_cast<uint32_t*>(base + o_keys);
   uint32_t* idx = reinterpret_cast<uint32_t*>(base + o_idx0);
   uint32_t* idx_alt = reinterpret_cast<uint32_t*>(base + o_idx1);
-  uint32_t* skeys = reinterpret_cast<uint32_t*>(base + o_sk0);
-  uint32_t* skeys_alt = reinterpret_cast<uint32_t*>(base + o_sk1);
+  unsigned long long* skeys = reinterpret_cast<unsigned long long*>(base + o_sk0);
+  unsigned long long* skeys_alt = reinterpret_cast<unsigned long long*>(base + o_sk1);
   Seg* cur = reinterpret_cast<Seg*>(base + o_seg0);
   Seg* nxt = reinterpret_cast<Seg*>(base + o_seg1);
-  uint32_t* sbeg = reinterpret_cast<uint32_t*>(base + o_beg);
-  uint32_t* send = reinterpret_cast<uint32_t*>(base + o_end);
+  uint32_t* red = reinterpret_cast<uint32_t*>(base + o_red);
+  int* axis = reinterpret_cast<int*>(base + o_axis);
   LNode* nodes = reinterpret_cast<LNode*>(base + o_nodes);
   float* lbounds = reinterpret_cast<float*>(base + o_lb);
   uint32_t* size = reinterpret_cast<uint32_t*>(base + o_size);
@@ -293,26 +378,39 @@ extern "C" int32_t sq_tree_build_d(sq_ctx* ctx, int32_t dim, uint32_t n, const f
   const uint32_t init[4] = {0, 1, 0, 0};
   CKB(cudaMemcpyAsync(ctr, init, sizeof(init), cudaMemcpyHostToDevice, st));
   std::vector<std::pair<uint32_t, uint32_t>> levels;  // level-order id ranges
+  // Positions fit in the keys' high word: a stable sort over bits
+  // [0, 32 + pos_bits) orders by (segment start, key).
+  int pos_bits = 1;
+  while (pos_bits < 32 && (uint64_t(1) << pos_bits) < n) ++pos_bits;
+  const int end_bit = 32 + pos_bits;
   uint32_t m = 1, made = 1;
+  uint64_t own_launches = 1;  // keys_kernel
+  uint64_t longest = n;  // bound on this level's longest segment (median splits halve it)
   while (m > 0) {
     levels.emplace_back(made - m, made);
     CKB(cudaMemsetAsync(ctr, 0, 4, st));      // next segments
-    CKB(cudaMemsetAsync(ctr + 2, 0, 4, st));  // sort segments
-    LevelParams p{d_prim_aabbs, D, n, keys, idx, cur, m, nxt, ctr, nodes, lbounds, sbeg, send, skeys};
-    if (m < 1024) level_kernel<256><<<m, 256, 0, st>>>(p);
-    else level_kernel<32><<<blocks_for(m, 8), 256, 0, st>>>(p);
+    CKB(cudaMemsetAsync(ctr + 2, 0, 4, st));  // split segments
+    place_keys_kernel<<<std::min<uint32_t>(blocks_for(n, 256), 148 * 8), 256, 0, st>>>(skeys, n);
+    LevelParams p{d_prim_aabbs, D, n, keys, idx, cur, m, nxt, ctr, nodes, lbounds, skeys, red, axis, 4096u};
+    own_launches += m >= kWide ? 2 : 5;
+    if (m >= kWide) {
+      level_kernel<32><<<blocks_for(m, 8), 256, 0, st>>>(p);
+    } else {
+      const dim3 grid(uint32_t(std::max<uint64_t>(1, (longest + p.chunk - 1) / p.chunk)), m);
+      red_init_kernel<<<blocks_for(uint64_t(m) * 4 * kMaxDim, 256), 256, 0, st>>>(red, m);
+      red_kernel<<<grid, 256, 0, st>>>(p);
+      decide_kernel<<<blocks_for(m, 128), 128, 0, st>>>(p);
+      split_keys_kernel<<<grid, 256, 0, st>>>(p);
+    }
     CKB(cudaGetLastError());
     uint32_t h[4];
     CKB(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st));
     CKB(cudaStreamSynchronize(st));
-    const uint32_t n_next = h[0], n_sort = h[2];
+    const uint32_t n_next = h[0], n_split = h[2];
     made = h[1];
-    if (n_sort > 0) {
-      // Positions outside the sorted segments keep their primitive.
-      CKB(cudaMemcpyAsync(idx_alt, idx, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
+    if (n_split > 0) {
       size_t need = 0;
-      CKB(cub::DeviceSegmentedSort::StableSortPairs(nullptr, need, skeys, skeys_alt, idx, idx_alt, int(n), int(n_sort),
-                                                    sbeg, send, st));
+      CKB(cub::DeviceRadixSort::SortPairs(nullptr, need, skeys, skeys_alt, idx, idx_alt, int(n), 0, end_bit, st));
       if (need > temp_cap) {
         if (temp) CKB(cudaFreeAsync(temp, st));
         temp = nullptr;
@@ -320,12 +418,12 @@ extern "C" int32_t sq_tree_build_d(sq_ctx* ctx, int32_t dim, uint32_t n, const f
         CKB(cudaMallocAsync(&temp, need, st));
         temp_cap = need;
       }
-      CKB(cub::DeviceSegmentedSort::StableSortPairs(temp, need, skeys, skeys_alt, idx, idx_alt, int(n), int(n_sort),
-                                                    sbeg, send, st));
+      CKB(cub::DeviceRadixSort::SortPairs(temp, need, skeys, skeys_alt, idx, idx_alt, int(n), 0, end_bit, st));
       std::swap(idx, idx_alt);
     }
     std::swap(cur, nxt);
     m = n_next;
+    longest = (longest + 1) / 2;
   }
   const uint32_t n_nodes = made;
   if (n_nodes > node_capacity) return done(fail(ctx, SQ_ERR_CAPACITY, "node_capacity too small"));
@@ -339,7 +437,7 @@ extern "C" int32_t sq_tree_build_d(sq_ctx* ctx, int32_t dim, uint32_t n, const f
                                                         d_child_b, d_prim_count);
   CKB(cudaGetLastError());
   CKB(cudaMemcpyAsync(d_prim_indices, idx, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
-  ctx->launches += 2 + 2 * levels.size() + 1;
+  ctx->launches += own_launches + 2 * levels.size() + 1;
   rc = done(SQ_OK);
   CK(cudaStreamSynchronize(st));
   *n_nodes_out = n_nodes;
