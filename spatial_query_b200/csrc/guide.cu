@@ -641,6 +641,23 @@ int* g_err_slot(sq_ctx* ctx) {
   return p;
 }
 
+}  // namespace
+
+// The context's error slot goes with the context (a later context at the
+// same address, possibly on another device, must not inherit it).
+void sqi::release_err_slot(sq_ctx* ctx) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  for (auto it = g_err_slots.begin(); it != g_err_slots.end(); ++it) {
+    if (it->first == ctx) {
+      cudaFree(it->second);
+      g_err_slots.erase(it);
+      return;
+    }
+  }
+}
+
+namespace {
+
 int32_t check_err(sq_ctx* ctx, int* err) {
   int h = 0;
   CK(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));

@@ -197,6 +197,7 @@ extern "C" int32_t sq_ctx_destroy(sq_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->own) cudaStreamSynchronize(ctx->own);
   if (ctx->lane) sq_ctx_destroy(ctx->lane);
+  sqi::release_err_slot(ctx);
   if (ctx->arena.p) cudaFree(ctx->arena.p);
   if (ctx->d_replays) cudaFree(ctx->d_replays);
   if (ctx->replay_list.p) cudaFree(ctx->replay_list.p);

@@ -120,6 +120,9 @@ int32_t rtc_kernel_set(uint32_t stride, const char* src, KernelSet* out, std::st
 // that lane's scratch. One chunk when n is small. Returns when every copy out
 // has landed.
 uint32_t pipeline_chunks(uint32_t n);
+// Frees the learned guide's per-context error flag (guide.cu); called when
+// the context is destroyed.
+void release_err_slot(sq_ctx* ctx);
 // ctx->lane, made on first use, with the context's traversal settings.
 int32_t second_lane(sq_ctx* ctx, sq_ctx** out);
 int32_t pipelined(sq_ctx* ctx, uint32_t n, const std::function<int32_t(uint32_t, uint32_t, cudaStream_t)>& in,
