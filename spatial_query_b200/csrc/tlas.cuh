@@ -589,8 +589,11 @@ __global__ void __launch_bounds__(kThreads, (IK == kInstMesh && !REF && !STATS) 
             uint32_t face;
             const float mts = fdiv(L.limit, s);
             uint32_t bflag = 0u;
+            // Only nearest queries are answered again when an instance's hit
+            // is not certified, so the others walk the BLAS in the crate's
+            // own order, whose answer needs no certificate.
             const bool bh = blas_nearest<REF>(p, __float_as_uint(rec[IL::blas]), lr, f && !isnan(mts), mts, s_code,
-                                              s_t, tid, L.sp, ts, face, nl, bflag, L.ref);
+                                              s_t, tid, L.sp, ts, face, nl, bflag, L.ref || !is_nearest());
             if (bh) {
               const float toi = fmul(ts, s);
               if (!(toi > L.limit)) {
