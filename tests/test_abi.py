@@ -1,7 +1,11 @@
-"""The C ABI library loads, exports every symbol include/sq.h declares, and
+"""The C ABI library loads, exports every symbol the headers under include/
+declare, fails loudly when it is missing (there is no CPU fallback), and
 behaves on a machine without a GPU (no compute call is made here)."""
+import glob
 import os
 import re
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -11,10 +15,12 @@ import spatial_query_b200 as sq
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_symbols():
-    text = open(os.path.join(ROOT, "include", "sq.h")).read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(sq_[a-z0-9_]+)\s*\(", text)))
+def declared_symbols(headers=None):
+    names = set()
+    for h in headers or sorted(glob.glob(os.path.join(ROOT, "include", "*.h"))):
+        text = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        names |= set(re.findall(r"\b(sq_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
 
 
 def test_header_declares_the_query_surface():
@@ -29,6 +35,24 @@ def test_library_exports_every_declared_symbol():
     missing = [s for s in declared_symbols() if not hasattr(lib, s)]
     assert not missing, missing
     assert set(declared_symbols()) <= set(sq.SIGNATURES)
+
+
+def test_every_header_is_covered():
+    heads = sorted(os.path.basename(h) for h in glob.glob(os.path.join(ROOT, "include", "*.h")))
+    assert heads == ["sq.h", "sq_guide.h"]
+    assert "sq_guide_create" in declared_symbols() and "sq_raycast_nearest_guided_d" in declared_symbols()
+
+
+def test_missing_library_raises():
+    code = ("import spatial_query_b200 as sq\n"
+            "sq.LIB_PATH = '/nonexistent/libsqcuda.so'\n"
+            "sq._lib = None\n"
+            "try:\n"
+            "    sq.lib()\n"
+            "except ImportError as e:\n"
+            "    print('raised', 'missing' in str(e))\n")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=120)
+    assert out.stdout.strip() == "raised True", out.stdout + out.stderr
 
 
 def test_version():
