@@ -55,6 +55,39 @@ def test_missing_library_raises():
     assert out.stdout.strip() == "raised True", out.stdout + out.stderr
 
 
+_NULL_PROBE = """
+import ctypes as C, sys
+import spatial_query_b200 as sq
+L = sq.lib()
+P = C.c_void_p
+v = int(sys.argv[1])
+bad = []
+calls = 0
+for name, (res, args) in sorted(sq.SIGNATURES.items()):
+    if res is not C.c_int32 or not args or args[0] is not P:
+        continue
+    vals = [float(v) if a in (C.c_float, C.c_double) else
+            v if a in (C.c_int32, C.c_uint32, C.c_int64, C.c_uint64, C.c_size_t) else None for a in args]
+    rc = getattr(L, name)(*vals)
+    calls += 1
+    if rc not in range(0, 8):
+        bad.append((name, rc))
+print(calls, bad)
+"""
+
+
+@pytest.mark.parametrize("size", [0, 1, 3])
+def test_null_handles_return_a_status(size):
+    """Every entry point that takes a handle, called with null handles and
+    pointers and small sizes, returns a status code instead of faulting
+    (a separate process, so that a crash names itself)."""
+    out = subprocess.run([sys.executable, "-c", _NULL_PROBE, str(size)], cwd=ROOT, capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    calls, bad = out.stdout.strip().split(" ", 1)
+    assert int(calls) >= 60 and bad == "[]", out.stdout
+
+
 def test_version():
     assert sq.lib().sq_version() == 1
 
