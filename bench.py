@@ -786,7 +786,8 @@ def main():
             "vs_baseline": None, "dtype": "f32 (traversal), bf16 x bf16 -> f32 (guide MLP)",
             "data": "synthetic (seeded height field and rays)",
             "config": {"workload": WORKLOAD,
-                       "path": "learned-seeded: fused tcgen05 MLP inference + seeded near-first traversal",
+                       "path": "learned-seeded: fused tcgen05 MLP inference + seeded near-first traversal "
+                               "(the two halves of the batch on two lanes)",
                        "identical_hits": identical,
                        "plain_gpu": {"value": round(plain_value, 3), "unit": "Mrays/s", "ms_per_step": round(plain_ms, 4),
                                      "path": "plain GPU traversal, autotuned: "
