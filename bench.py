@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--epochs", type=int, default=8, help="guide training epochs (batch 8192, AdamW lr 1e-3)")
     ap.add_argument("--rays", type=int, default=1 << 20,
                     help="rays per step (half coherent, half incoherent); the metric is quoted at 1,048,576")
+    ap.add_argument("--side-configs", type=int, default=1,
+                    help="terrain, one GPU: also run the 10,000-box, two-level and D = 6 workloads and fold their "
+                         "results into the line (0: skip)")
     return ap.parse_args()
 
 
@@ -370,11 +373,11 @@ def bench_instanced(args):
                        "gpu_launches_per_frame": int(per_frame_launches)},
             "cpu_baseline": cpu_all, "cpu_1thread": cpu_one,
             "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
     graph.close()
     g.close()
     blas.close()
     ctx.close()
+    return line
 
 
 def bench_boxes(args):
@@ -418,9 +421,9 @@ def bench_boxes(args):
                        "identical_to_cpu": same, "l2": "flushed between steps", "learned_guide": learned},
             "cpu_baseline": cpu_all, "cpu_1thread": cpu_one,
             "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
     scene.close()
     ctx.close()
+    return line
 
 
 def learned_boxes(args, scene, ctx, stream, flush, s, d_rays, leaf, toi, plain_ms):
@@ -467,12 +470,18 @@ def learned_boxes(args, scene, ctx, stream, flush, s, d_rays, leaf, toi, plain_m
         raise SystemExit("learned-seeded hits differ from the plain query's")
     hit = d_lt >= 0
     top1 = float((d_bucket[hit] == d_lt[hit]).float().mean().item())
+    st_p = guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], g_leaf, g_toi, d_bucket=d_lt, stats=True)
+    torch.cuda.synchronize()
+    if not (torch.equal(g_leaf, leaf) and torch.equal(g_toi.view(torch.int32), toi.view(torch.int32))):
+        raise SystemExit("true-bucket seeded hits differ from the plain query's")
+    perfect = lambda: guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], g_leaf, g_toi, d_bucket=d_lt)
     for _ in range(args.warmup):
         guided()
     torch.cuda.synchronize()
     g_ms = sum(timed(stream, guided, args.steps, flush)) / args.steps
     pr_ms = sum(timed(stream, predict, args.steps, flush)) / args.steps
     sd_ms = sum(timed(stream, seeded, args.steps, flush)) / args.steps
+    pf_ms = sum(timed(stream, perfect, args.steps, flush)) / args.steps
     guide.close()
     return {"value": round(n / g_ms / 1000.0, 3), "unit": "Mrays/s", "ms_per_step": round(g_ms, 4),
             "learned_vs_plain": round(plain_ms / g_ms, 4), "hit_id_agreement": agree, "identical_hits": identical,
@@ -480,6 +489,10 @@ def learned_boxes(args, scene, ctx, stream, flush, s, d_rays, leaf, toi, plain_m
             "inference_tflops": round(2 * (MLP_MACS - 128 * (4096 - gi["n_out"])) * n / (pr_ms / 1000) / 1e12, 1),
             "nodes_visited_per_ray": {"plain": round(st["nodes_visited"] / n, 2),
                                       "seeded": round(st_g["nodes_visited"] / n, 2)},
+            "perfect_seed": {"what": "the seeded walk given the true bucket of every ray (misses: no seed), the "
+                                     "upper bound of any guide", "nodes_visited_per_ray": round(st_p["nodes_visited"] / n, 2),
+                             "narrow_tests_per_ray": round(st_p["narrow_tests"] / n, 2),
+                             "seeded_traversal_ms": round(pf_ms, 4), "plain_traversal_ms": round(plain_ms, 4)},
             "buckets": gi["n_buckets"], "outputs": gi["n_out"], "bucket_depth": depth, "top1_accuracy": round(top1, 4),
             "training": {"rays": n_train, "epochs": args.epochs, "batch": 8192, "optimizer": "AdamW lr 1e-3",
                          "seconds": round(train_s, 2), "final_loss": round(float(losses[-1]), 4),
@@ -535,9 +548,28 @@ def bench_mixture(args):
                        "l2": "flushed between steps"},
             "cpu_baseline": cpu_all, "cpu_1thread": cpu_one,
             "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
     scene.close()
     ctx.close()
+    return line
+
+
+def side_configs(args):
+    """The other benchmark configurations, each run as its own --workload
+    line would run it, folded into the headline line: value, time, CPU
+    baseline and exactness per configuration."""
+    out = {}
+    for name, fn in (("boxes_10k_config1", bench_boxes), ("instanced_config3", bench_instanced),
+                     ("mixture_d6_config4", bench_mixture)):
+        line = fn(args)
+        c = line["config"]
+        entry = {"metric": line["metric"], "value": line["value"], "unit": line["unit"],
+                 "ms_per_step": line["ms_per_step"], "cpu_baseline": line["cpu_baseline"],
+                 "cpu_1thread": line["cpu_1thread"], "clocks": line["clocks"]}
+        for k in ("identical_to_cpu", "learned_guide", "overlap", "mqueries_per_s", "queries_per_frame"):
+            if k in c:
+                entry[k] = c[k]
+        out[name] = entry
+    return out
 
 
 def main():
@@ -548,7 +580,8 @@ def main():
         return
     if args.workload != "terrain":
         if rank == 0:
-            {"boxes": bench_boxes, "instanced": bench_instanced, "mixture": bench_mixture}[args.workload](args)
+            line = {"boxes": bench_boxes, "instanced": bench_instanced, "mixture": bench_mixture}[args.workload](args)
+            print(json.dumps(line), flush=True)
         return
 
     import ctypes as C
@@ -589,18 +622,21 @@ def main():
     d_bucket = torch.empty(n, dtype=torch.int32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
-    # The same tree built on the device (sq_tree_build_d), timed on the host
-    # clock (it synchronises once per tree level), checked against the host tree.
+    # The same tree built on the device (sq_tree_build_d), timed with CUDA
+    # events on the context's stream (median of 5 after a warm build),
+    # checked against the host tree.
     d_aabbs = torch.from_numpy(geom.world_aabbs()).to(dev)
     n_prims = geom.leaf_count
     sq.tree_build_d(ctx, 3, d_aabbs, n_prims)
     torch.cuda.synchronize(dev)
     dev_build = []
-    for _ in range(3):
-        t0 = time.perf_counter()
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
         dt_arrays = sq.tree_build_d(ctx, 3, d_aabbs, n_prims)
-        torch.cuda.synchronize(dev)
-        dev_build.append(time.perf_counter() - t0)
+        e1.record(stream)
+        e1.synchronize()
+        dev_build.append(e0.elapsed_time(e1))
     b_, ca_, cb_, pc_, pi_ = (t.cpu().numpy() for t in dt_arrays)
     same_tree = (np.array_equal(b_, tree.bounds) and np.array_equal(ca_.view(np.uint32), tree.child_a)
                  and np.array_equal(cb_.view(np.uint32), tree.child_b)
@@ -656,7 +692,16 @@ def main():
     torch.cuda.synchronize()
     hit = d_lt >= 0
     top1 = float((d_bucket[hit] == d_lt[hit]).float().mean().item())
-    del d_lt
+    # The upper bound of any guide: the seeded walk given every ray's true
+    # bucket (the bucket of its plain nearest hit; misses get no seed).
+    p_leaf, p_toi, p_nrm = torch.empty_like(d_leaf), torch.empty_like(d_toi), torch.empty_like(d_nrm)
+    st_p = guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], p_leaf, p_toi, p_nrm, d_bucket=d_lt, stats=True)
+    torch.cuda.synchronize()
+    if not (torch.equal(p_leaf, d_leaf) and torch.equal(p_toi.view(torch.int32), d_toi.view(torch.int32))):
+        raise SystemExit("true-bucket seeded hits differ from the plain query's")
+
+    def perfect():
+        guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], p_leaf, p_toi, p_nrm, d_bucket=d_lt)
 
     def record_bytes(stats):
         fetches = (stats["nodes_visited"] - n) // 2  # child-pair records read
@@ -682,6 +727,7 @@ def main():
     p_ms = timed(stream, plain, args.steps, flush)
     pr_ms = timed(stream, predict, args.steps, flush)
     sd_ms = timed(stream, seeded, args.steps, flush)
+    pf_ms = timed(stream, perfect, args.steps, flush)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -698,6 +744,7 @@ def main():
     allhits()
     al_ms = timed(stream, allhits, args.steps, flush)
     ms, plain_ms, predict_ms, seeded_ms = mean_max(g_ms), mean_max(p_ms), mean_max(pr_ms), mean_max(sd_ms)
+    perfect_ms = mean_max(pf_ms)
     all_ms = mean_max(al_ms)
     value = world * n / (ms / 1000) / 1e6
     plain_value = world * n / (plain_ms / 1000) / 1e6
@@ -814,6 +861,19 @@ def main():
                                         "plain_traversal": round(plain_ms, 4)},
                        "nodes_visited_per_ray": {"plain": round(st["nodes_visited"] / n, 3),
                                                  "learned_seeded": round(st_g["nodes_visited"] / n, 3)},
+                       "perfect_seed": {"what": "the seeded walk given the true bucket of every ray (misses: no "
+                                                "seed), the upper bound of any guide",
+                                        "nodes_visited_per_ray": round(st_p["nodes_visited"] / n, 3),
+                                        "narrow_tests_per_ray": round(st_p["narrow_tests"] / n, 3),
+                                        "seeded_traversal_ms": round(perfect_ms, 4),
+                                        "plain_traversal_ms": round(plain_ms, 4)},
+                       "learned_vs_plain_bound": {
+                           "mlp_ms_at_peak": round(mlp_flop / (tpeak[0] * 1e12) * 1000, 4),
+                           "plain_ms": round(plain_ms, 4),
+                           "best_possible": round(plain_ms / (mlp_flop / (tpeak[0] * 1e12) * 1000 + perfect_ms), 4),
+                           "what": "learned-seeded time >= the network's FLOPs at the tensor peak + the true-bucket "
+                                   "seeded walk; its ratio to the plain walk bounds learned_vs_plain for this "
+                                   "network on this workload"},
                        "guide": {"buckets": guide.info()["n_buckets"], "train_rays": n_train,
                                  "epochs": args.epochs, "batch": guide.batch, "optimizer": "AdamW lr 1e-3",
                                  "loss_per_epoch": [round(float(x), 4) for x in losses],
@@ -821,10 +881,13 @@ def main():
                                  "replayed_in_reference_order": int(replayed_g)},
                        "l2": "flushed between steps (256 MiB write, outside the timed events)",
                        "parallelism": f"replicated scene, rays sharded per rank (dp{world})",
-                       "tree_build": {"host_s": round(host_build_s, 3), "device_ms": round(min(dev_build) * 1e3, 2),
+                       "tree_build": {"host_s": round(host_build_s, 3),
+                                      "device_ms": round(statistics.median(dev_build), 2),
+                                      "device_ms_all": [round(x, 2) for x in dev_build],
                                       "identical": bool(same_tree),
                                       "what": "tree::build on 1,048,576 triangle AABBs: host restatement "
-                                              "(all cores) vs sq_tree_build_d (host clock, best of 3)"},
+                                              "(all cores, host clock) vs sq_tree_build_d (CUDA events on the "
+                                              "context's stream, median of 5)"},
                        "tree": {"nodes": info["n_nodes"], "depth": info["max_depth"],
                                 "node_record_bytes": info["node_record_bytes"],
                                 "prim_record_bytes": info["prim_record_bytes"]}},
@@ -841,6 +904,8 @@ def main():
             line["cpu_baseline"] = cpu
         if f64:
             line["config"]["f64_reference"] = f64
+        if world == 1 and args.side_configs:
+            line["config"]["other_configs"] = side_configs(args)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -335,10 +335,12 @@ int32_t sq_overlap_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_regions, uin
  * loads the library, held until the process exits). n beyond that returns
  * SQ_ERR_CAPACITY, as does a result larger than leaf_capacity (*total is then
  * set). Device pointers; runs on `stream` (a cudaStream_t, NULL = the legacy
- * default stream) and returns when the results are written. The first call
- * on a device looks up the array's address on that device: make that first
- * call before any stream capture. Every call shares the one array, so calls
- * that overlap on the GPU (from several threads or streams) race. With no
+ * default stream) and returns when the results are written: every call reads
+ * the total back and waits for its stream, so it blocks the calling thread
+ * and must never be called on a stream that is being captured. The first
+ * call on a device also looks up the array's address on that device. Every
+ * call shares the one array, so calls that overlap on the GPU (from several
+ * threads or streams) race. With no
  * sort scratch, each region's leaves are kept ascending by insertion as they
  * are found: a region with k results costs O(k^2) writes (sq_overlap and
  * sq_overlap_d append, then sort every segment at once). */

@@ -697,6 +697,8 @@ struct sq_guide {
   bool images_fresh = false;
   // buckets
   uint2* d_buckets = nullptr;
+  uint32_t* d_bucket_sibs = nullptr;  // per bucket, sib_stride ancestor-sibling slots
+  uint32_t sib_stride = 0;
   int32_t* d_bucket_of_id = nullptr;
   // batch scratch
   uint32_t B = 0;
@@ -724,17 +726,26 @@ int32_t galloc(sq_guide* g, void** p, size_t bytes) {
   return SQ_OK;
 }
 
-// Buckets: the nodes at cfg.depth (and leaves above it), in preorder.
-void build_buckets(const sq_bvh* b, uint32_t depth, std::vector<uint2>& table, std::vector<uint32_t>& starts) {
+// Buckets: the nodes at cfg.depth (and leaves above it), in preorder. Per
+// bucket also the slots (record << 1 | slot) of its ancestors' other
+// children, root level first, `stride` = depth entries (kNoHit past the
+// bucket's own depth): with the bucket they partition the tree, so a walk
+// that starts in the bucket and then takes them covers every leaf once.
+void build_buckets(const sq_bvh* b, uint32_t depth, std::vector<uint2>& table, std::vector<uint32_t>& starts,
+                   std::vector<uint32_t>& sibs, uint32_t stride) {
   table.clear();
   starts.clear();
+  sibs.clear();
   if (b->n_nodes == 0) return;
   struct Item { uint32_t node, depth, parent_slot; };
   std::vector<Item> stack{{0u, 0u, kNoHit}};
+  std::vector<uint32_t> path;  // sibling slot per level of the current item's ancestors
   while (!stack.empty()) {
     const Item it = stack.back();
     stack.pop_back();
     const uint32_t i = it.node;
+    path.resize(it.depth);
+    if (it.depth > 0) path[it.depth - 1] = it.parent_slot ^ 1u;  // the other child of the same record
     const bool leaf = b->h_count[i] != 0;
     if (leaf || it.depth == depth) {
       const uint32_t code = leaf ? (kLeafBit | b->h_child_a[i]) : b->h_iidx[i];
@@ -742,6 +753,7 @@ void build_buckets(const sq_bvh* b, uint32_t depth, std::vector<uint2>& table, s
       uint32_t k = i;
       while (b->h_count[k] == 0) k = b->h_child_a[k];
       starts.push_back(b->h_child_a[k]);
+      for (uint32_t s = 0; s < stride; ++s) sibs.push_back(s < path.size() ? path[s] : kNoHit);
       continue;
     }
     const uint32_t rec = b->h_iidx[i];
@@ -898,6 +910,15 @@ int32_t adam_step(sq_guide* g) {
   return refresh_bf16(g);
 }
 
+sqi::SeedTable seed_table(const sq_guide* g) {
+  sqi::SeedTable t;
+  t.buckets = g->d_buckets;
+  t.sibs = g->d_bucket_sibs;
+  t.n_buckets = g->n_buckets;
+  t.sib_stride = g->sib_stride;
+  return t;
+}
+
 int32_t predict(sq_guide* g, const float* d_rays, uint32_t n, int32_t* d_bucket) {
   sq_ctx* ctx = g->ctx;
   if (n == 0) return SQ_OK;
@@ -974,8 +995,9 @@ extern "C" int32_t sq_guide_create(sq_ctx* ctx, const sq_bvh* b, const sq_guide_
   g->cfg = c;
   g->B = c.batch;
   std::vector<uint2> table;
-  std::vector<uint32_t> starts;
-  build_buckets(b, c.depth, table, starts);
+  std::vector<uint32_t> starts, sibs;
+  g->sib_stride = std::max<uint32_t>(c.depth, 1u);
+  build_buckets(b, c.depth, table, starts, sibs, g->sib_stride);
   g->n_buckets = uint32_t(table.size());
   g->n_out = (g->n_buckets + 127) / 128 * 128;
   if (g->n_out > 4096) return fail(ctx, SQ_ERR_INVALID, "more than 4096 buckets: lower the depth");
@@ -1010,7 +1032,8 @@ extern "C" int32_t sq_guide_create(sq_ctx* ctx, const sq_bvh* b, const sq_guide_
       (rc = A(&g->W3bT, kHidden * kHidden * 2)) || (rc = A(&g->W4bT, NO * kHidden * 2)) ||
       (rc = A(&g->w1_img, 16384)) || (rc = A(&g->w23_img, 2 * kChunkBytes)) ||
       (rc = A(&g->w4_img, NO / 128 * kChunkBytes)) || (rc = A(&g->infer_bias, (384 + NO) * 4)) ||
-      (rc = A(&g->d_buckets, table.size() * sizeof(uint2))) || (rc = A(&g->d_bucket_of_id, size_t(b->n_prims) * 4)) ||
+      (rc = A(&g->d_buckets, table.size() * sizeof(uint2))) || (rc = A(&g->d_bucket_sibs, sibs.size() * 4)) ||
+      (rc = A(&g->d_bucket_of_id, size_t(b->n_prims) * 4)) ||
       (rc = A(&g->X, B * kInPad * 2)) || (rc = A(&g->XT, size_t(kHidden) * B * 2)) ||
       (rc = A(&g->Z, B * std::max<size_t>(NO, kHidden) * 4)) || (rc = A(&g->dZ4, B * NO * 2)) ||
       (rc = A(&g->dZ4T, B * NO * 2)) || (rc = A(&g->dZ, B * kHidden * 2)) || (rc = A(&g->dZT, B * kHidden * 2)) ||
@@ -1030,6 +1053,7 @@ extern "C" int32_t sq_guide_create(sq_ctx* ctx, const sq_bvh* b, const sq_guide_
   CK(cudaMemset(g->XT, 0, size_t(kHidden) * B * 2));
   // bucket table and per-primitive buckets
   CK(cudaMemcpy(g->d_buckets, table.data(), table.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(g->d_bucket_sibs, sibs.data(), sibs.size() * 4, cudaMemcpyHostToDevice));
   {
     uint32_t* d_starts = nullptr;
     CK(cudaMalloc(&d_starts, starts.size() * 4));
@@ -1248,8 +1272,7 @@ extern "C" int32_t sq_raycast_nearest_guided_d(sq_ctx* ctx, const sq_bvh* b, con
       g->ctx = on;
       rc = predict(g, d_rays + size_t(s0) * 6, m, d + s0);
       g->ctx = saved;
-      if (!rc) rc = seeded_nearest(on, b, d_rays + size_t(s0) * 6, m, max_toi, d + s0, g->d_buckets, g->n_buckets, c,
-                                   nullptr);
+      if (!rc) rc = seeded_nearest(on, b, d_rays + size_t(s0) * 6, m, max_toi, d + s0, seed_table(g), c, nullptr);
       if (rc) failed = on;
     }
     // The context's stream takes the lane's half back in every case.
@@ -1270,7 +1293,7 @@ extern "C" int32_t sq_raycast_nearest_guided_d(sq_ctx* ctx, const sq_bvh* b, con
     if (rc) return rc;
     seeds = d;
   }
-  return seeded_nearest(ctx, b, d_rays, n, max_toi, seeds, g->d_buckets, g->n_buckets, *out, stats);
+  return seeded_nearest(ctx, b, d_rays, n, max_toi, seeds, seed_table(g), *out, stats);
 }
 
 extern "C" int32_t sq_raycast_nearest_guided(sq_ctx* ctx, const sq_bvh* b, const sq_guide* gc, const float* rays,
@@ -1316,7 +1339,7 @@ extern "C" int32_t sq_raycast_nearest_guided(sq_ctx* ctx, const sq_bvh* b, const
     if (c.sub_object) c.sub_object += s0;
     if (c.normal) c.normal += size_t(s0) * 3;
     if (c.point) c.point += size_t(s0) * 3;
-    return seeded_nearest(lane, b, d_q + size_t(s0) * 6, m, max_toi, d_b + s0, g->d_buckets, g->n_buckets, c, nullptr);
+    return seeded_nearest(lane, b, d_q + size_t(s0) * 6, m, max_toi, d_b + s0, seed_table(g), c, nullptr);
   };
   auto out = [&](uint32_t s0, uint32_t m, cudaStream_t sm) -> int32_t {
     auto cp = [&](void* dst, const void* src, size_t per) -> int32_t {

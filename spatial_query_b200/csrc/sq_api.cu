@@ -1015,7 +1015,6 @@ struct NoAllocDevice {
   bool ready = false;
   uint32_t* scratch = nullptr;  // device address of g_noalloc_scratch on this device
   int sm_count = 0;
-  int blocks_per_sm = 1;
 };
 
 constexpr int kNoAllocMaxDevices = 64;
@@ -1023,37 +1022,49 @@ NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
 std::mutex g_noalloc_mu;
 
 // Exclusive prefix sum of n counts into offsets[0..n], offsets[n] = total, in
-// one block (n <= kNoAllocMaxRegions): each thread sums a contiguous run, the
-// block scans the run totals, each thread writes its run.
+// one block (n <= kNoAllocMaxRegions) and no scratch beyond shared memory:
+// tiles of 1,024 consecutive counts (one per thread, so the loads coalesce)
+// are scanned block-wide (warp shuffles, then the 32 warp totals), and the
+// running total carries from tile to tile.
 __global__ void __launch_bounds__(1024) noalloc_scan_kernel(const uint32_t* counts, unsigned long long* offsets,
                                                             uint32_t n) {
-  __shared__ unsigned long long part[1024];
-  const uint32_t t = threadIdx.x;
-  const uint32_t per = (n + 1023u) / 1024u;
-  const uint32_t lo = min(n, t * per), hi = min(n, lo + per);
-  unsigned long long s = 0;
-  for (uint32_t i = lo; i < hi; ++i) s += counts[i];
-  part[t] = s;
-  __syncthreads();
-  for (uint32_t off = 1; off < 1024; off <<= 1) {
-    const unsigned long long v = t >= off ? part[t - off] : 0ull;
+  __shared__ unsigned long long warp_sum[32];
+  constexpr unsigned FULL = 0xffffffffu;
+  const uint32_t t = threadIdx.x, lane = t & 31u, w = t >> 5;
+  unsigned long long carry = 0;
+  for (uint32_t base = 0; base < n; base += 1024u) {
+    const uint32_t i = base + t;
+    const unsigned long long v = i < n ? counts[i] : 0ull;
+    unsigned long long x = v;  // inclusive scan within the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(FULL, x, o);
+      if (lane >= uint32_t(o)) x += y;
+    }
+    if (lane == 31u) warp_sum[w] = x;
     __syncthreads();
-    part[t] += v;
+    if (w == 0) {
+      unsigned long long s = warp_sum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(FULL, s, o);
+        if (lane >= uint32_t(o)) s += y;
+      }
+      warp_sum[lane] = s;  // inclusive over warps
+    }
     __syncthreads();
+    if (i < n) offsets[i] = carry + (w ? warp_sum[w - 1] : 0ull) + (x - v);
+    carry += warp_sum[31];
+    __syncthreads();  // warp_sum is rewritten by the next tile
   }
-  unsigned long long base = part[t] - s;  // exclusive
-  for (uint32_t i = lo; i < hi; ++i) {
-    offsets[i] = base;
-    base += counts[i];
-  }
-  if (t == 1023) offsets[n] = part[1023];
+  if (t == 0) offsets[n] = carry;
 }
 
 }  // namespace
 
 // The device address of the static scratch, looked up once per device (with
 // that device current) by the first call on it.
-static int32_t noalloc_setup(int device, const void* overlap_fn, NoAllocDevice** out) {
+static int32_t noalloc_setup(int device, NoAllocDevice** out) {
   if (device < 0 || device >= kNoAllocMaxDevices) return SQ_ERR_INVALID;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   NoAllocDevice& d = g_noalloc_dev[device];
@@ -1064,12 +1075,10 @@ static int32_t noalloc_setup(int device, const void* overlap_fn, NoAllocDevice**
       cudaGetLastError();
       return SQ_ERR_CUDA;
     }
-    int sms = 0, bps = 0;
+    int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return SQ_ERR_CUDA;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, overlap_fn, kThreads, 0) != cudaSuccess || bps < 1) bps = 1;
     d.scratch = static_cast<uint32_t*>(ptr);
     d.sm_count = sms;
-    d.blocks_per_sm = bps;
     d.ready = true;
   }
   *out = &d;
@@ -1083,7 +1092,7 @@ extern "C" int32_t sq_overlap_noalloc(const sq_bvh* b, const float* d_regions, u
   if (n > kNoAllocMaxRegions) return SQ_ERR_CAPACITY;  // beyond the static scratch
   if (!b->ks.overlap) return SQ_ERR_UNSUPPORTED;
   NoAllocDevice* d = nullptr;
-  int32_t rc = noalloc_setup(b->device, b->ks.overlap, &d);
+  int32_t rc = noalloc_setup(b->device, &d);
   if (rc) return rc;
   if (cudaSetDevice(b->device) != cudaSuccess) return SQ_ERR_CUDA;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1093,13 +1102,18 @@ extern "C" int32_t sq_overlap_noalloc(const sq_bvh* b, const float* d_regions, u
   if (cudaMemsetAsync(counts, 0, (size_t(n) + 1) * sizeof(uint32_t), s) != cudaSuccess ||
       cudaMemsetAsync(counters, 0, kNoAllocCounters * sizeof(uint32_t), s) != cudaSuccess)
     return SQ_ERR_CUDA;
-  const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(d->sm_count) * d->blocks_per_sm,
-                                                                  (uint64_t(n) + kThreads - 1) / kThreads));
   const int stack = int(std::max<uint32_t>(b->depth, 1));
   const size_t smem = size_t(stack) * kThreads * 8;
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(b->ks.overlap, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
     return SQ_ERR_CUDA;
+  // The persistent grid: the blocks of this scene's overlap kernel (its D,
+  // narrow phase, consumer code) that fit at once with this tree's stack.
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, b->ks.overlap, kThreads, smem) != cudaSuccess || bps < 1)
+    bps = 1;
+  const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(d->sm_count) * bps,
+                                                                  (uint64_t(n) + kThreads - 1) / kThreads));
   if (b->n_nodes != 0 && n != 0) {
     QueryParams p;
     base_params(b, f, p);
@@ -1113,7 +1127,17 @@ extern "C" int32_t sq_overlap_noalloc(const sq_bvh* b, const float* d_regions, u
     if (cudaLaunchKernel(b->ks.overlap, dim3(unsigned(grid)), dim3(kThreads), args, smem, s) != cudaSuccess)
       return SQ_ERR_CUDA;
   }
-  noalloc_scan_kernel<<<1, 1024, 0, s>>>(counts, reinterpret_cast<unsigned long long*>(d_offsets), n);
+  {
+    // Launched with cudaLaunchKernel so its status is this launch's own (a
+    // stale error of the caller's earlier work is neither reported nor cleared).
+    const uint32_t* c_counts = counts;
+    unsigned long long* c_offsets = reinterpret_cast<unsigned long long*>(d_offsets);
+    uint32_t c_n = n;
+    void* args[] = {&c_counts, &c_offsets, &c_n};
+    if (cudaLaunchKernel(reinterpret_cast<const void*>(noalloc_scan_kernel), dim3(1), dim3(1024), args, 0, s) !=
+        cudaSuccess)
+      return SQ_ERR_CUDA;
+  }
   unsigned long long tot = 0;
   if (cudaMemcpyAsync(&tot, d_offsets + n, sizeof(tot), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
@@ -1136,7 +1160,7 @@ extern "C" int32_t sq_overlap_noalloc(const sq_bvh* b, const float* d_regions, u
     if (cudaLaunchKernel(b->ks.overlap, dim3(unsigned(grid)), dim3(kThreads), args, smem, s) != cudaSuccess)
       return SQ_ERR_CUDA;
   }
-  if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return SQ_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return SQ_ERR_CUDA;
   return SQ_OK;
 }
 
@@ -1145,8 +1169,7 @@ extern "C" int32_t sq_overlap_noalloc(const sq_bvh* b, const float* d_regions, u
 // ============================================================================
 
 int32_t sqi::seeded_nearest(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, uint32_t n, float max_toi,
-                            const int32_t* d_bucket, const uint2* d_buckets, uint32_t n_buckets, const sq_hits& o,
-                            sq_query_stats* st) {
+                            const int32_t* d_bucket, const SeedTable& seeds, const sq_hits& o, sq_query_stats* st) {
   int32_t rc = check_scene(ctx, b);
   if (rc) return rc;
   if (!o.leaf || (n && (!d_rays || !d_bucket))) return fail(ctx, SQ_ERR_INVALID, "null argument");
@@ -1166,10 +1189,14 @@ int32_t sqi::seeded_nearest(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, u
     p.out_normal = o.normal;
     p.out_point = o.point;
     p.seed_bucket = d_bucket;
-    p.buckets = d_buckets;
-    p.n_buckets = n_buckets;
+    p.buckets = seeds.buckets;
+    p.bucket_sibs = seeds.sibs;
+    p.n_buckets = seeds.n_buckets;
+    p.sib_stride = seeds.sib_stride;
     if (st) p.stats = ctx->d_stats;
-    // one stack entry more than the depth: the root waits below the bucket
+    // The bucket's ancestors' other children wait on the stack (one per level
+    // above the bucket) while the bucket is searched: no deeper than a plain
+    // descent to the same node, so the tree's depth bounds the stack.
     if ((rc = near_first_launch(ctx, b, b->ks.ray_nearest_seeded[st ? 1 : 0], b->ks.ray_nearest[1][st ? 1 : 0], p,
                                 b->depth + 1)))
       return rc;

@@ -133,10 +133,20 @@ int32_t pipelined(sq_ctx* ctx, uint32_t n, const std::function<int32_t(uint32_t,
 // (sq_api.cu): the fill passes append in walk order.
 int32_t sort_csr_segments(sq_ctx* ctx, uint32_t* d_leaves, uint64_t total, const uint64_t* d_offsets, uint32_t n);
 
+// The learned guide's buckets on the device: per bucket its node code and
+// the slot of its box (parent record << 1 | slot, kNoHit for the root), and
+// the slots of its ancestors' other children, root level first, sib_stride
+// per bucket (kNoHit past the bucket's depth).
+struct SeedTable {
+  const uint2* buckets = nullptr;
+  const uint32_t* sibs = nullptr;
+  uint32_t n_buckets = 0;
+  uint32_t sib_stride = 0;
+};
+
 // Learned-seeded nearest rays (sq_api.cu): enqueues the SEED kernel.
 int32_t seeded_nearest(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, uint32_t n, float max_toi,
-                       const int32_t* d_bucket, const uint2* d_buckets, uint32_t n_buckets, const sq_hits& o,
-                       sq_query_stats* st);
+                       const int32_t* d_bucket, const SeedTable& seeds, const sq_hits& o, sq_query_stats* st);
 
 inline int32_t fail(sq_ctx* c, int32_t code, const std::string& msg) {
   if (c) c->err = msg;

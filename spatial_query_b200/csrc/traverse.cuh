@@ -114,7 +114,9 @@ struct QueryParams {
   const float* root_box;  // min[D], max[D] of the root (device memory: refit updates it)
   const int32_t* seed_bucket;  // learned guide: predicted bucket per query (seeded launches)
   const uint2* buckets;        // per bucket: node code, parent record << 1 | slot (kNoHit: the root)
+  const uint32_t* bucket_sibs; // per bucket, sib_stride slots (record << 1 | slot) of its ancestors' other children
   uint32_t n_buckets;
+  uint32_t sib_stride;
   const int* nonfinite;   // non-zero when some node bound is not finite (device memory)
   float max_toi;
   int stack;              // traversal-stack entries per thread (dynamic shared memory)
@@ -322,7 +324,6 @@ template <int D, int K> struct Lane {
   uint32_t best_pos; // near-first: primitive position of the best hit (for its certification)
   uint32_t q;
   uint32_t code;
-  uint32_t skip;     // seeded: the bucket subtree already searched first
   int sp;
   bool fast;
   uint32_t best_leaf;
@@ -341,9 +342,12 @@ template <int D, int K> struct Lane {
 // child (Aila and Laine's while-while loop with dynamic fetch).
 //
 // SEED (nearest rays only): the learned guide's predicted bucket, a subtree
-// at a fixed depth, is searched first; its nearest hit becomes the limit
-// for the rest of the walk from the root, which skips that subtree. The
-// answer is certified exactly as in near-first, so it is the reference's.
+// at a fixed depth, is searched first; its nearest hit becomes the limit for
+// the rest of the tree, which is exactly the other children of the bucket's
+// ancestors: they wait on the stack from the start and are walked after the
+// bucket (no ancestor's record is read twice, so a right seed never costs
+// more box tests than the plain walk). The answer is certified exactly as in
+// near-first, so it is the reference's whatever the seed.
 // WIDE (near-first nearest rays, no counters, no seed): the walk reads the
 // four-wide records; a step tests up to four children, goes to the nearest
 // and stacks the others farthest first.
@@ -504,7 +508,6 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
       hi[i] = p.root_box[D + i];
     }
     float te;
-    L.skip = kNoHit;
     const bool hit_root = test_box(lo, hi, te);
     if constexpr (SEED) {
       const int32_t bk = p.seed_bucket[q];
@@ -520,14 +523,36 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
             blo[i] = box[i];
             bhi[i] = box[D + i];
           }
+          if (STATS) L.v_nodes += 1;
           if (test_box(blo, bhi, tb)) {
-            // The root waits below the bucket; the bucket goes first.
-            s_code[tid] = p.root_code;
-            s_t[tid] = te;
-            L.sp = 1;
+            // The bucket goes first. The siblings of its ancestors wait on
+            // the stack, the root's child deepest, so the bucket's nearest
+            // neighbours in the tree come up first; each is tested against
+            // the ray now and against the (shrunk) limit when popped. Their
+            // records are independent loads, not a dependent descent.
+            const uint32_t* sibs = p.bucket_sibs + size_t(bk) * p.sib_stride;
+            for (uint32_t i = 0; i < p.sib_stride; ++i) {
+              const uint32_t sl = __ldg(sibs + i);
+              if (sl == kNoHit) break;
+              float rec[NL::vec * 4];
+              load_vec<NL::vec>(p.nodes + size_t(sl >> 1) * NL::vec, rec);
+              const bool second = (sl & 1u) != 0u;
+              float slo[D], shi[D];
+#pragma unroll
+              for (int k = 0; k < D; ++k) {
+                slo[k] = second ? rec[2 * D + k] : rec[k];
+                shi[k] = second ? rec[3 * D + k] : rec[D + k];
+              }
+              const uint32_t sc = __float_as_uint(second ? rec[4 * D + 1] : rec[4 * D]);
+              float ts;
+              if (STATS) L.v_nodes += 1;
+              if (test_box(slo, shi, ts)) {
+                s_code[L.sp * kThreads + tid] = sc;
+                s_t[L.sp * kThreads + tid] = ts;
+                ++L.sp;
+              }
+            }
             L.code = e.x;
-            L.skip = e.x;
-            if (STATS) L.v_nodes += 1;
           }
         }
       }
@@ -724,8 +749,8 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
         const uint32_t ca = __float_as_uint(rec[4 * D]);
         const uint32_t cb = __float_as_uint(rec[4 * D + 1]);
         float ta, tb;
-        const bool pa = test_box(rec, rec + D, ta) && (!SEED || ca != L.skip);
-        const bool pb = test_box(rec + 2 * D, rec + 3 * D, tb) && (!SEED || cb != L.skip);
+        const bool pa = test_box(rec, rec + D, ta);
+        const bool pb = test_box(rec + 2 * D, rec + 3 * D, tb);
         if (STATS) L.v_nodes += 2;
         if constexpr (K == kOverlap) {
           // A region heavier than the budget goes to the warp-per-region

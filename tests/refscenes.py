@@ -103,3 +103,35 @@ def line_balls(n: int, radius: float) -> np.ndarray:
 
 def axis_ray() -> np.ndarray:
     return np.array([0, 0, 0, 1, 0, 0], np.float32)
+
+
+def cube_mesh(size: float) -> np.ndarray:
+    """A cube of edge `size` centred on the origin, two triangles per face
+    (tris[12, 9]): the mesh of viewport-lib's primitives::cube(size) that the
+    known-answer tests of crates/viewport-lib-query/src/lib.rs:338-431 put
+    under their instances (that crate is absent, so its triangulation is
+    restated here; the tests' answers depend only on the cube's faces)."""
+    h = np.float32(size) * np.float32(0.5)
+    tris = []
+    for axis in range(3):
+        u, v = (axis + 1) % 3, (axis + 2) % 3
+        for side in (-h, h):
+            quad = []
+            for a, b in ((-h, -h), (h, -h), (h, h), (-h, h)):
+                p = [np.float32(0)] * 3
+                p[axis], p[u], p[v] = side, a, b
+                quad.append(p)
+            tris.append(quad[0] + quad[1] + quad[2])
+            tris.append(quad[0] + quad[2] + quad[3])
+    return np.asarray(tris, dtype=np.float32)
+
+
+def mesh_instances(trans, scale=None):
+    """(rot, trans, scale, blas_id) of identity-rotation instances of one mesh
+    (Mat4::from_translation / from_scale_rotation_translation with an identity
+    quaternion, lib.rs:357, 381-382, 396, 410-418)."""
+    trans = np.asarray(trans, dtype=np.float32).reshape(-1, 3)
+    n = trans.shape[0]
+    rot = np.repeat(np.eye(3, dtype=np.float32)[None], n, axis=0)
+    s = np.ones(n, np.float32) if scale is None else np.asarray(scale, dtype=np.float32).reshape(n)
+    return rot, trans, s, np.zeros(n, np.uint32)

@@ -173,7 +173,7 @@ def mesh_pair(s):
 @pytest.fixture(scope="module")
 def small_instanced():
     s = scenes.instanced_scene(seed=7, n_instances=256, n_blas=4, n_rays=20000, n_casts=4096, n_regions=4096,
-                               n_frames=3, blas_lo=2000, blas_hi=20000)
+                               n_frames=12, blas_lo=2000, blas_hi=20000)
     return (s,) + mesh_pair(s)
 
 
@@ -237,19 +237,31 @@ def test_mixed_launch_and_graph_frames(small_instanced):
     mixed()
     check(o)
     # A frame: add this frame's N(0,1) steps to every translation, refit, query.
+    # The graph reads the steps from one device buffer; before each replay the
+    # frame's own steps are copied into it on the context's stream, so every
+    # replay moves the instances by a different amount and the translations
+    # accumulate across replays, as the benchmark's 100 frames do.
+    delta = torch.empty_like(steps[0])
     trans = s["trans"].copy()
     with torch.cuda.stream(stream):
+        delta.copy_(steps[0])
         c.graph_begin()
-        g.refit_d(d_delta=steps[0])
+        g.refit_d(d_delta=delta)
         mixed()
         graph = c.graph_end()
-    for f in range(1):
+    n_frames = s["frame_steps"].shape[0]
+    assert n_frames >= 10
+    for f in range(n_frames):
+        with torch.cuda.stream(stream):
+            delta.copy_(steps[f])
         graph.launch()
-        trans = trans + s["frame_steps"][0]
+        trans = trans + s["frame_steps"][f]
         o.refit(trans)
         check(o)
-    nb, wa = g.read_bounds()
-    assert np.array_equal(nb, o.tree()["bounds"])
+        nb, wa = g.read_bounds()
+        ot = o.tree()
+        assert np.array_equal(nb, ot["bounds"]), f"frame {f}: node bounds differ from the oracle's refit"
+        assert np.array_equal(wa, ot["world_aabbs"]), f"frame {f}: instance world AABBs differ"
     graph.close()
 
 
@@ -263,3 +275,49 @@ def test_instanced_full_nearest():
     assert_same_nearest(o.shapecast_nearest(s["casts"], s["cast_len"]),
                         g.shapecast_nearest(s["casts"], s["cast_len"]), label="instanced casts")
     assert_same_csr(o.overlap(s["regions"]), g.overlap(s["regions"]), label="instanced overlaps")
+
+
+# -- crates/viewport-lib-query/src/lib.rs:338-431 on the device ----------------
+
+def _cube_pair(trans, scale=None):
+    from refscenes import cube_mesh, mesh_instances
+    cube = cube_mesh(2.0)
+    rot, t, sc, bid = mesh_instances(trans, scale)
+    oblas = O.BlasSet(np.array([0, cube.shape[0]], np.uint64), cube)
+    o = O.TlasScene("mesh", 3, rot, t, sc, blas_id=bid, blas=oblas)
+    blas = sq.BlasSet(ctx(), [cube])
+    g = sq.DeviceTlas(ctx(), "mesh", 3, rot, t, sc, blas_id=bid, blas=blas)
+    return oblas, o, blas, g
+
+
+@pytest.mark.parametrize("case", ["face_and_id", "nearest_wins", "away_misses", "scaled_world_toi"])
+def test_viewport_mesh_known_answers(case, order):
+    """The four mesh-instance tests of viewport-lib-query (lib.rs:338-431)
+    through the device's mesh instances: the reference's answers hold, and
+    every field equals the oracle's bit for bit."""
+    ray = lambda d: ray_new(np.zeros(3, np.float32), np.asarray(d, np.float32))[None]
+    if case == "face_and_id":
+        keep = _cube_pair([[5.0, 0.0, 0.0]])
+        r = ray([1, 0, 0])
+    elif case == "nearest_wins":
+        keep = _cube_pair([[10.0, 0.0, 0.0], [5.0, 0.0, 0.0]])
+        r = ray([1, 0, 0])
+    elif case == "away_misses":
+        keep = _cube_pair([[5.0, 0.0, 0.0]])
+        r = ray([-1, 0, 0])
+    else:
+        keep = _cube_pair([[20.0, 0.0, 0.0]], scale=[3.0])
+        r = ray([1, 0, 0])
+    _, o, _, g = keep
+    ref = o.nearest(r, 100.0)
+    got = g.raycast_nearest(r, 100.0)
+    assert_same_nearest(ref, got, label=case)
+    if case == "face_and_id":
+        assert got.leaf[0] == 0 and abs(float(got.toi[0]) - 4.0) < 1e-3 and abs(float(got.normal[0, 0])) > 0.9
+        assert got.sub_object[0] < 12
+    elif case == "nearest_wins":
+        assert [100, 200][got.leaf[0]] == 200
+    elif case == "away_misses":
+        assert got.leaf[0] == O.NO_HIT
+    else:
+        assert got.leaf[0] == 0 and abs(float(got.toi[0]) - 17.0) < 1e-2

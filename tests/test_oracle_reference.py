@@ -467,3 +467,50 @@ def test_gpu_suite_scenes_hit_and_miss():
     rays = conformance_rays(2000, 0x0BAD_F00D_1111_2222, -30.0, 30.0, -6.0, 6.0)
     h = sc.nearest(rays, 200.0)
     assert np.any(h.leaf != NO) and np.any(h.leaf == NO)
+
+
+# -- crates/viewport-lib-query/src/lib.rs (mesh instances, ray_triangle) -------
+
+def _cube_tlas(trans, scale=None):
+    from refscenes import cube_mesh, mesh_instances
+    cube = cube_mesh(2.0)
+    rot, t, s, bid = mesh_instances(trans, scale)
+    blas = O.BlasSet(np.array([0, cube.shape[0]], np.uint64), cube)
+    return O.TlasScene("mesh", 3, rot, t, s, blas_id=bid, blas=blas), blas
+
+
+def test_ray_hits_registered_cube_with_face_and_id():
+    """lib.rs:338-366: a cube of edge 2 at x = 5; a +x ray from the origin hits
+    its near face at toi 4 (within 1e-3) with a normal along x and a face
+    sub-object; the instance is the one registered (pick id 42)."""
+    pick_ids = np.array([42], np.uint32)
+    sc, _ = _cube_tlas([[5.0, 0.0, 0.0]])
+    h = sc.nearest(ray_new(np.zeros(3, np.float32), np.array([1, 0, 0], np.float32))[None], 100.0)
+    assert h.leaf[0] != NO and pick_ids[h.leaf[0]] == 42
+    assert abs(float(h.toi[0]) - (5.0 + -1.0)) < 1e-3
+    assert abs(float(h.normal[0, 0])) > 0.9
+    assert h.sub[0] != NO and h.sub[0] < 12  # a face of the 12-triangle cube
+
+
+def test_nearest_instance_wins():
+    """lib.rs:368-380: cubes at x = 10 (pick 100) and x = 5 (pick 200): 200."""
+    pick_ids = np.array([100, 200], np.uint32)
+    sc, _ = _cube_tlas([[10.0, 0.0, 0.0], [5.0, 0.0, 0.0]])
+    h = sc.nearest(ray_new(np.zeros(3, np.float32), np.array([1, 0, 0], np.float32))[None], 100.0)
+    assert h.leaf[0] != NO and pick_ids[h.leaf[0]] == 200
+
+
+def test_ray_pointing_away_misses():
+    """lib.rs:382-392: a -x ray from the origin misses the cube at x = 5."""
+    sc, _ = _cube_tlas([[5.0, 0.0, 0.0]])
+    h = sc.nearest(ray_new(np.zeros(3, np.float32), np.array([-1, 0, 0], np.float32))[None], 100.0)
+    assert h.leaf[0] == NO
+
+
+def test_scaled_instance_reports_world_distance():
+    """lib.rs:394-430: the cube scaled 3x at x = 20: world toi 20 + 3 * -1 = 17
+    (within 1e-2), not the local-space distance."""
+    sc, _ = _cube_tlas([[20.0, 0.0, 0.0]], scale=[3.0])
+    h = sc.nearest(ray_new(np.zeros(3, np.float32), np.array([1, 0, 0], np.float32))[None], 100.0)
+    assert h.leaf[0] == 0
+    assert abs(float(h.toi[0]) - 17.0) < 1e-2
