@@ -60,7 +60,7 @@ extern "C" {
 #define SQ_NARROW_AABB 0        /* leaf = box min[D],max[D]; hit = slab entry (maths/aabb.rs:118-148) */
 #define SQ_NARROW_SPHERE 1      /* leaf = centre[D],radius; near root, far root from inside (tests/differential.rs:61-82) */
 #define SQ_NARROW_SPHERE_NEAR 2 /* leaf = centre[D],radius; near root only (tests/gpu.rs:92-106) */
-#define SQ_NARROW_TRIANGLE 3    /* leaf = v0,v1,v2 (D = 3); Moeller-Trumbore (viewport-lib-query/src/lib.rs:295-320) */
+#define SQ_NARROW_TRIANGLE 3    /* leaf = v0,v1,v2 (D = 3); Moeller-Trumbore (viewport-lib-query/src/lib.rs:281-306) */
 #define SQ_NARROW_CUSTOM 4      /* a consumer narrow phase compiled at run time (sq_bvh_upload_custom) */
 
 /* Traversal order of nearest queries (sq_ctx_set_order). */
@@ -76,6 +76,10 @@ extern "C" {
 #define SQ_LAYOUT_WIDE 1        /* four-wide records (the binary tree with every other level folded into
                                    its parent): half the dependent fetches per ray, twice the boxes per
                                    fetch; the autotuner picks it where it is faster */
+#define SQ_LAYOUT_QUANT 2       /* the four-wide records quantised: each child box as 8-bit steps from
+                                   the record's corner, rounded outward (64 B per record at D = 3, as a
+                                   child-pair record); the exact records serve scenes with non-finite
+                                   bounds */
 
 typedef struct sq_ctx sq_ctx;
 typedef struct sq_bvh sq_bvh;
@@ -157,8 +161,9 @@ int32_t sq_ctx_set_replay_window(sq_ctx* ctx, float window);
  * configuration on a sample of device-resident rays (CUDA events, best of
  * `reps`), keeps the fastest in the context and reports the table. The knobs
  * are the traversal order (near-first, certified / the reference's order,
- * both give the reference's hits) and the persistent grid's resident blocks
- * per SM (0 = the occupancy limit). No counterpart in the reference, whose
+ * both give the reference's hits), the node records near-first walks
+ * (child-pair, four-wide, quantised four-wide) and the persistent grid's
+ * resident blocks per SM (0 = the occupancy limit): up to 32 entries. No counterpart in the reference, whose
  * WGSL path has a fixed 64-thread workgroup (gpu/mod.rs:119-227). */
 typedef struct sq_tune_entry {
   int32_t order;
@@ -228,6 +233,47 @@ int32_t sq_raycast_nearest_f64(sq_ctx* ctx, const sq_bvh* bvh, const double* ray
 int32_t sq_raycast_nearest_f64_d(sq_ctx* ctx, const sq_bvh* bvh, const double* d_rays, uint32_t n, double max_toi,
                                  const double* d_max_toi_per_query, const sq_filter* filter, uint32_t* d_leaf,
                                  double* d_toi, double* d_normal, sq_query_stats* stats);
+
+/* Bounded sorted hit lists of an f64 scene (as sq_hit_lists, with double
+ * toi and normals; no sub-objects: f64 scenes carry none). */
+typedef struct sq_hit_lists_f64 {
+  uint32_t k;
+  uint32_t* count;  /* [n] full number of hits */
+  uint32_t* leaf;   /* [n*k] */
+  double* toi;      /* [n*k] */
+  double* normal;   /* [n*k*D] or NULL */
+} sq_hit_lists_f64;
+
+/* raycast_all / raycast_crossings (accel/bvh.rs:196-328) with Scalar = f64,
+ * walked in the crate's own order; crossings != 0 lists both roots of sphere
+ * leaves (tests/crossings.rs:505-521), one crossing per hit otherwise. The
+ * first min(count, k) entries per ray equal the f64 CPU path's sorted list. */
+int32_t sq_raycast_all_f64(sq_ctx* ctx, const sq_bvh* bvh, const double* rays, uint32_t n, double max_toi,
+                           const double* max_toi_per_query, const sq_filter* filter, int32_t crossings,
+                           const sq_hit_lists_f64* out);
+int32_t sq_raycast_all_f64_d(sq_ctx* ctx, const sq_bvh* bvh, const double* d_rays, uint32_t n, double max_toi,
+                             const double* d_max_toi_per_query, const sq_filter* filter, int32_t crossings,
+                             const sq_hit_lists_f64* d_out);
+/* shapecast_nearest / shapecast_all (accel/bvh.rs:330-414) with Scalar = f64:
+ * casts are origin[D], dir[D], probe.min[D], probe.max[D] (doubles); the same
+ * narrow phases as sq_shapecast_*. */
+int32_t sq_shapecast_nearest_f64(sq_ctx* ctx, const sq_bvh* bvh, const double* casts, uint32_t n, double max_toi,
+                                 const double* max_toi_per_query, const sq_filter* filter, uint32_t* leaf, double* toi,
+                                 double* normal);
+int32_t sq_shapecast_nearest_f64_d(sq_ctx* ctx, const sq_bvh* bvh, const double* d_casts, uint32_t n, double max_toi,
+                                   const double* d_max_toi_per_query, const sq_filter* filter, uint32_t* d_leaf,
+                                   double* d_toi, double* d_normal);
+int32_t sq_shapecast_all_f64(sq_ctx* ctx, const sq_bvh* bvh, const double* casts, uint32_t n, double max_toi,
+                             const double* max_toi_per_query, const sq_filter* filter, const sq_hit_lists_f64* out);
+int32_t sq_shapecast_all_f64_d(sq_ctx* ctx, const sq_bvh* bvh, const double* d_casts, uint32_t n, double max_toi,
+                               const double* d_max_toi_per_query, const sq_filter* filter,
+                               const sq_hit_lists_f64* d_out);
+/* overlap (accel/bvh.rs:416-456) of double regions lo[D], hi[D] as CSR, as
+ * sq_overlap / sq_overlap_d. */
+int32_t sq_overlap_f64(sq_ctx* ctx, const sq_bvh* bvh, const double* regions, uint32_t n, const sq_filter* filter,
+                       uint64_t* offsets, uint32_t* leaves, uint64_t leaf_capacity, uint64_t* total);
+int32_t sq_overlap_f64_d(sq_ctx* ctx, const sq_bvh* bvh, const double* d_regions, uint32_t n, const sq_filter* filter,
+                         uint64_t* d_offsets, uint32_t* d_leaves, uint64_t leaf_capacity, uint64_t* total);
 
 /* ---- scene upload (GpuRaycaster::new, gpu/mod.rs:252-303) -------------------
  * Takes the host tree as tree::Node arrays (accel/tree.rs:21-26; Bvh::nodes
@@ -306,7 +352,15 @@ int32_t sq_raycast_crossings_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_ra
                                const float* d_max_toi_per_query, const sq_filter* filter, const sq_hit_lists* d_out);
 
 /* shapecast_nearest / shapecast_all (accel/bvh.rs:330-414). The point of a
- * cast hit is cast.at(toi) (query/shapecast.rs:61-63). */
+ * cast hit is cast.at(toi) (query/shapecast.rs:61-63). Narrow phases: boxes
+ * are the exact swept-box test (the slab against the leaf box grown by the
+ * probe, ShapeCast::broadphase, shapecast.rs:70-73); balls sweep the probe's
+ * max[0] as a radius (tests/shape_overlap.rs:96-110). The reference defines
+ * no swept box against a triangle, so a triangle leaf answers the swept box
+ * against the triangle's AABB (the same broadphase slab, the normal of the
+ * AABB face entered): a conservative time of impact, never later than the
+ * exact swept-box-vs-triangle one. Mesh instances of a Tlas likewise answer
+ * a cast against the instance's world AABB. */
 int32_t sq_shapecast_nearest(sq_ctx* ctx, const sq_bvh* bvh, const float* casts, uint32_t n, float max_toi,
                              const float* max_toi_per_query, const sq_filter* filter, const sq_hits* out);
 int32_t sq_shapecast_nearest_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_casts, uint32_t n, float max_toi,

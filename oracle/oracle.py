@@ -49,8 +49,8 @@ def lib():
         L.orc_scene_stats.argtypes = [P, P, P]
         L.orc_nearest.argtypes = [P, i32, u32, P, P, f32, u64, i64, i32, P, P, P, P, P, P, P]
         L.orc_all.argtypes = [P, i32, i32, u32, P, P, f32, u64, i64, i32, u32, P, P, P, P, P, P, P]
-        L.orc_shapecast_nearest.argtypes = [P, i32, u32, P, P, f32, u64, i64, i32, P, P, P, P, P]
-        L.orc_shapecast_all.argtypes = [P, i32, u32, P, P, f32, u64, i64, i32, u32, P, P, P, P, P]
+        L.orc_shapecast_nearest.argtypes = [P, i32, u32, P, P, f32, u64, i64, i32, P, P, P, P, P, P]
+        L.orc_shapecast_all.argtypes = [P, i32, u32, P, P, f32, u64, i64, i32, u32, P, P, P, P, P, P]
         L.orc_overlap.argtypes = [P, i32, u32, P, u64, i64, i32, P, P, P]
         L.orc_ray_intersect.argtypes = [i32, P, P, f32, P, P]
         L.orc_normalize.argtypes = [i32, u32, P]
@@ -104,10 +104,10 @@ class Hits:
 class HitLists:
     """All-hits results: count (full), and the first k entries per query."""
 
-    def __init__(self, n, k, dim):
+    def __init__(self, n, k, dim, f64=False):
         self.count = np.empty(n, np.uint32)
         self.leaf = np.empty((n, k), np.uint32)
-        self.toi = np.empty((n, k), np.float32)
+        self.toi = np.empty((n, k), np.float64 if f64 else np.float32)
         self.normal = np.empty((n, k, dim), np.float32)
         self.sub = np.empty((n, k), np.uint32)
         self.stats = None
@@ -174,11 +174,13 @@ class Scene:
         n = rays.shape[0]
         per = np.ndim(max_toi) > 0
         mt = _f32(max_toi) if per else None
-        h = HitLists(n, k, self.dim)
+        f64 = self.prec == 64
+        h = HitLists(n, k, self.dim, f64)
         st = np.empty((n, 4), np.uint64) if stats else None
         lib().orc_all(self.h, 1 if naive else 0, 1 if crossings else 0, n, _p(rays), _p(mt),
                       0.0 if per else float(max_toi), mask, exclude, threads or default_threads(), k, _p(h.count),
-                      _p(h.leaf), _p(h.toi), None, _p(h.normal), _p(h.sub), _p(st))
+                      _p(h.leaf), None if f64 else _p(h.toi), _p(h.toi) if f64 else None, _p(h.normal), _p(h.sub),
+                      _p(st))
         h.stats = st
         return h
 
@@ -188,10 +190,12 @@ class Scene:
         n = casts.shape[0]
         per = np.ndim(max_toi) > 0
         mt = _f32(max_toi) if per else None
-        h = Hits(n, self.dim)
+        f64 = self.prec == 64
+        h = Hits(n, self.dim, f64)
         lib().orc_shapecast_nearest(self.h, 1 if naive else 0, n, _p(casts), _p(mt), 0.0 if per else float(max_toi),
-                                    mask, exclude, threads or default_threads(), _p(h.leaf), _p(h.toi),
-                                    _p(h.normal), _p(h.point), _p(h.sub))
+                                    mask, exclude, threads or default_threads(), _p(h.leaf),
+                                    None if f64 else _p(h.toi), _p(h.toi) if f64 else None, _p(h.normal),
+                                    _p(h.point), _p(h.sub))
         return h
 
     def shapecast_all(self, casts, max_toi, k=16, mask=0xFFFFFFFFFFFFFFFF, exclude=-1, naive=False,
@@ -200,10 +204,11 @@ class Scene:
         n = casts.shape[0]
         per = np.ndim(max_toi) > 0
         mt = _f32(max_toi) if per else None
-        h = HitLists(n, k, self.dim)
+        f64 = self.prec == 64
+        h = HitLists(n, k, self.dim, f64)
         lib().orc_shapecast_all(self.h, 1 if naive else 0, n, _p(casts), _p(mt), 0.0 if per else float(max_toi),
-                                mask, exclude, threads or default_threads(), k, _p(h.count), _p(h.leaf), _p(h.toi),
-                                _p(h.normal), _p(h.sub))
+                                mask, exclude, threads or default_threads(), k, _p(h.count), _p(h.leaf),
+                                None if f64 else _p(h.toi), _p(h.toi) if f64 else None, _p(h.normal), _p(h.sub))
         return h
 
     def overlap(self, regions, mask=0xFFFFFFFFFFFFFFFF, exclude=-1, naive=False, threads=None):

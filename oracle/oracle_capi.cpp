@@ -300,8 +300,8 @@ int orc_all(void* h, int mode, int crossings, uint32_t nq, const float* rays, co
 
 // Nearest shape cast (bvh.rs:331-375 / naive.rs:131-158).
 int orc_shapecast_nearest(void* h, int mode, uint32_t nq, const float* casts, const float* max_toi_arr, float max_toi,
-                          uint64_t mask, int64_t exclude, int threads, uint32_t* leaf, float* toi, float* normal,
-                          float* point, uint32_t* sub) {
+                          uint64_t mask, int64_t exclude, int threads, uint32_t* leaf, float* toi, double* toi64,
+                          float* normal, float* point, uint32_t* sub) {
   auto* b = static_cast<SceneBase*>(h);
   Filter f = make_filter(mask, exclude);
   auto run = [&](auto tag) -> int {
@@ -313,7 +313,8 @@ int orc_shapecast_nearest(void* h, int mode, uint32_t nq, const float* casts, co
           ShapeCast<DD, S> c = load_cast<DD, S>(casts + q * 4 * DD);
           S mt = S(max_toi_arr ? max_toi_arr[q] : max_toi);
           auto hit = mode == 0 ? s->bvh.shapecast_nearest(s->g, c, mt, f) : naive::shapecast_nearest<DD, S>(s->g, c, mt, f);
-          store_hit<DD, S, float>(hit, q, leaf, toi, normal, point, sub);
+          if (toi64) store_hit<DD, S, double>(hit, q, leaf, toi64, normal, point, sub);
+          else store_hit<DD, S, float>(hit, q, leaf, toi, normal, point, sub);
         }
       });
     });
@@ -325,7 +326,7 @@ int orc_shapecast_nearest(void* h, int mode, uint32_t nq, const float* casts, co
 // All shape-cast contacts (bvh.rs:378-414 / naive.rs:161-181).
 int orc_shapecast_all(void* h, int mode, uint32_t nq, const float* casts, const float* max_toi_arr, float max_toi,
                       uint64_t mask, int64_t exclude, int threads, uint32_t k, uint32_t* count, uint32_t* leaf,
-                      float* toi, float* normal, uint32_t* sub) {
+                      float* toi, double* toi64, float* normal, uint32_t* sub) {
   auto* b = static_cast<SceneBase*>(h);
   Filter f = make_filter(mask, exclude);
   auto run = [&](auto tag) -> int {
@@ -339,7 +340,8 @@ int orc_shapecast_all(void* h, int mode, uint32_t nq, const float* casts, const 
           S mt = S(max_toi_arr ? max_toi_arr[q] : max_toi);
           if (mode == 0) s->bvh.shapecast_all(s->g, c, mt, f, hits);
           else naive::shapecast_all<DD, S>(s->g, c, mt, f, hits);
-          store_list<DD, S, float>(hits, q, k, count, leaf, toi, normal, sub);
+          if (toi64) store_list<DD, S, double>(hits, q, k, count, leaf, toi64, normal, sub);
+          else store_list<DD, S, float>(hits, q, k, count, leaf, toi, normal, sub);
         }
       });
     });

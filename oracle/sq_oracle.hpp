@@ -388,7 +388,7 @@ template <int D, class S> inline Point<D, S> entry_normal(const Point<D, S>& dir
   return n;
 }
 
-// Moeller-Trumbore, double-sided (crates/viewport-lib-query/src/lib.rs:295-320),
+// Moeller-Trumbore, double-sided (crates/viewport-lib-query/src/lib.rs:281-306),
 // with glam Vec3's dot = (x*x' + y*y') + z*z' and cross component order.
 template <class S> struct V3 { S x, y, z; };
 template <class S> inline V3<S> v3sub(V3<S> a, V3<S> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }

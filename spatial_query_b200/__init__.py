@@ -38,6 +38,7 @@ SQ_ERR_COMPILE = 7
 NO_HIT = 0xFFFFFFFF
 LAYOUT_BINARY = 0
 LAYOUT_WIDE = 1
+LAYOUT_QUANT = 2
 NO_SUB = 0xFFFFFFFF
 
 NARROW = {"boxes": 0, "aabb": 0, "balls": 1, "sphere": 1, "balls_near": 2, "sphere_near": 2, "tris": 3,
@@ -56,6 +57,10 @@ class SqError(RuntimeError):
 
 class _Filter(C.Structure):
     _fields_ = [("layer_mask", C.c_uint64), ("exclude", C.c_int64)]
+
+
+class _Lists64(C.Structure):
+    _fields_ = [("k", C.c_uint32), ("count", P), ("leaf", P), ("toi", P), ("normal", P)]
 
 
 class _Hits(C.Structure):
@@ -110,6 +115,14 @@ SIGNATURES = {
                                       P, P]),
     "sq_raycast_nearest_f64": (C.c_int32, [P, P, P, C.c_uint32, C.c_double, P, P, P, P, P, P]),
     "sq_raycast_nearest_f64_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_double, P, P, P, P, P, P]),
+    "sq_raycast_all_f64": (C.c_int32, [P, P, P, C.c_uint32, C.c_double, P, P, C.c_int32, P]),
+    "sq_raycast_all_f64_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_double, P, P, C.c_int32, P]),
+    "sq_shapecast_nearest_f64": (C.c_int32, [P, P, P, C.c_uint32, C.c_double, P, P, P, P, P]),
+    "sq_shapecast_nearest_f64_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_double, P, P, P, P, P]),
+    "sq_shapecast_all_f64": (C.c_int32, [P, P, P, C.c_uint32, C.c_double, P, P, P]),
+    "sq_shapecast_all_f64_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_double, P, P, P]),
+    "sq_overlap_f64": (C.c_int32, [P, P, P, C.c_uint32, P, P, P, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "sq_overlap_f64_d": (C.c_int32, [P, P, P, C.c_uint32, P, P, P, C.c_uint64, C.POINTER(C.c_uint64)]),
     "sq_autotune_nearest_d": (C.c_int32, [P, P, P, C.c_uint32, C.c_float, C.c_uint32, P]),
     "sq_bvh_upload_custom": (C.c_int32, [P, C.c_uint32, P, P, P, P, C.c_uint32, P, P, C.c_uint32, P, C.c_char_p,
                                          C.POINTER(P)]),
@@ -377,7 +390,7 @@ class Context:
         self.check(lib().sq_ctx_set_order(self.h, order), "set_order")
 
     def set_layout(self, layout: int):
-        """LAYOUT_BINARY (default) or LAYOUT_WIDE node records for near-first rays."""
+        """LAYOUT_BINARY (default), LAYOUT_WIDE or LAYOUT_QUANT node records for near-first rays."""
         self.check(lib().sq_ctx_set_layout(self.h, layout), "set_layout")
 
     def set_replay_window(self, window: float):
@@ -741,6 +754,61 @@ class DeviceBvh64:
         sd = None if st is None else dict(nodes_visited=st.nodes_visited, aabb_tests=st.aabb_tests,
                                           narrow_tests=st.narrow_tests, hits=st.hits)
         return Hits(leaf, toi, nrm, None, None, sd)
+
+    def _limits(self, max_toi):
+        per = np.ndim(max_toi) > 0
+        return (0.0 if per else float(max_toi)), (np.ascontiguousarray(max_toi, dtype=np.float64) if per else None)
+
+    def _lists(self, fn, q, width, max_toi, k, mask, exclude, extra=()):
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, width * self.dim)
+        n = q.shape[0]
+        mt0, mt = self._limits(max_toi)
+        out = HitLists(np.empty(n, np.uint32), np.full((n, k), NO_HIT, np.uint32), np.zeros((n, k), np.float64),
+                       np.zeros((n, k, self.dim), np.float64))
+        o = _Lists64(k, _p(out.count), _p(out.leaf), _p(out.toi), _p(out.normal))
+        self.ctx.check(getattr(lib(), fn)(self.ctx.h, self.h, _p(q), n, mt0, _p(mt), _filter(mask, exclude), *extra,
+                                          C.byref(o)), fn)
+        return out
+
+    def raycast_all(self, rays, max_toi, k=16, mask=None, exclude=None) -> "HitLists":
+        """raycast_all with Scalar = f64: the first k hits per ray in hit order, full counts."""
+        return self._lists("sq_raycast_all_f64", rays, 2, max_toi, k, mask, exclude, (0,))
+
+    def raycast_crossings(self, rays, max_toi, k=16, mask=None, exclude=None) -> "HitLists":
+        return self._lists("sq_raycast_all_f64", rays, 2, max_toi, k, mask, exclude, (1,))
+
+    def shapecast_all(self, casts, max_toi, k=16, mask=None, exclude=None) -> "HitLists":
+        """casts: [n, 4D] doubles (origin, dir, probe.min, probe.max)."""
+        return self._lists("sq_shapecast_all_f64", casts, 4, max_toi, k, mask, exclude)
+
+    def shapecast_nearest(self, casts, max_toi, mask=None, exclude=None) -> Hits:
+        casts = np.ascontiguousarray(casts, dtype=np.float64).reshape(-1, 4 * self.dim)
+        n = casts.shape[0]
+        mt0, mt = self._limits(max_toi)
+        leaf = np.empty(n, np.uint32)
+        toi = np.empty(n, np.float64)
+        nrm = np.empty((n, self.dim), np.float64)
+        self.ctx.check(lib().sq_shapecast_nearest_f64(self.ctx.h, self.h, _p(casts), n, mt0, _p(mt),
+                                                      _filter(mask, exclude), _p(leaf), _p(toi), _p(nrm)),
+                       "sq_shapecast_nearest_f64")
+        return Hits(leaf, toi, nrm, None, None, None)
+
+    def overlap(self, regions, mask=None, exclude=None, capacity=None):
+        """CSR (offsets[n+1] u64, leaves u32) of double regions [n, 2D], leaves ascending per region."""
+        regions = np.ascontiguousarray(regions, dtype=np.float64).reshape(-1, 2 * self.dim)
+        n = regions.shape[0]
+        cap = capacity if capacity is not None else max(4 * n, 1024)
+        while True:
+            offsets = np.empty(n + 1, np.uint64)
+            leaves = np.empty(max(cap, 1), np.uint32)
+            total = C.c_uint64(0)
+            rc = lib().sq_overlap_f64(self.ctx.h, self.h, _p(regions), n, _filter(mask, exclude), _p(offsets),
+                                      _p(leaves), cap, C.byref(total))
+            if rc == SQ_ERR_CAPACITY and total.value > cap:
+                cap = int(total.value)
+                continue
+            self.ctx.check(rc, "sq_overlap_f64")
+            return offsets, leaves[: int(total.value)]
 
 
 class GpuRaycaster:

@@ -40,6 +40,7 @@ void base_params(const sq_bvh* b, const sq_filter* f, QueryParams& p) {
   p.nonfinite = b->d_nonfinite;
   p.root_code = b->root_code;
   p.wnodes = b->d_wnodes;
+  p.qnodes = b->d_qnodes;
   p.wroot = b->wroot;
   p.mask = f ? f->layer_mask : ~0ull;
   p.exclude = f ? f->exclude : -1;
@@ -92,6 +93,8 @@ int32_t nearest_core(sq_ctx* ctx, const sq_bvh* b, bool cast, const float* d_q, 
   // at most three children, so the stack holds 3 x (four-wide depth) + 1.
   if (!cast && !stats && ctx->layout == SQ_LAYOUT_WIDE && b->n_wide && b->ks.ray_nearest_wide)
     return near_first_launch(ctx, b, b->ks.ray_nearest_wide, ref_fn, p, 3 * b->wdepth + 1);
+  if (!cast && !stats && ctx->layout == SQ_LAYOUT_QUANT && b->n_wide && b->d_qnodes && b->ks.ray_nearest_quant)
+    return near_first_launch(ctx, b, b->ks.ray_nearest_quant, ref_fn, p, 3 * b->wdepth + 1);
   return near_first_launch(ctx, b, near_fn, ref_fn, p, b->depth);
 }
 
@@ -233,7 +236,8 @@ extern "C" int32_t sq_ctx_set_order(sq_ctx* ctx, int32_t order) {
 }
 
 extern "C" int32_t sq_ctx_set_layout(sq_ctx* ctx, int32_t layout) {
-  if (!ctx || (layout != SQ_LAYOUT_BINARY && layout != SQ_LAYOUT_WIDE)) return SQ_ERR_INVALID;
+  if (!ctx || (layout != SQ_LAYOUT_BINARY && layout != SQ_LAYOUT_WIDE && layout != SQ_LAYOUT_QUANT))
+    return SQ_ERR_INVALID;
   ctx->layout = layout;
   return SQ_OK;
 }
@@ -454,6 +458,25 @@ static int32_t upload_impl(sq_ctx* ctx, int32_t dim, int32_t narrow, uint32_t n_
     b->wroot = 0;
     b->wdepth = wdepth;
   }
+  // The quantised copies of the four-wide records (the kernels that walk them).
+  std::vector<uint32_t> qnodes;
+  if (b->n_wide && ks.ray_nearest_quant) {
+    const uint32_t WV = wide_vec(D), QV = quant_vec(D);
+    qnodes.assign(size_t(b->n_wide) * QV * 4, 0u);
+    for (uint32_t r = 0; r < b->n_wide; ++r) {
+      const float* rec = wnodes.data() + size_t(r) * WV * 4;
+      uint32_t codes[4];
+      std::memcpy(codes, rec + 8 * D, sizeof(codes));
+      uint32_t* out = qnodes.data() + size_t(r) * QV * 4;
+      switch (D) {
+        case 2: quantize_record<2>(rec, codes, out); break;
+        case 3: quantize_record<3>(rec, codes, out); break;
+        case 4: quantize_record<4>(rec, codes, out); break;
+        case 6: quantize_record<6>(rec, codes, out); break;
+        default: break;
+      }
+    }
+  }
 
   auto up = [&](void** dst, const void* src, size_t bytes) -> int32_t {
     CK(cudaMalloc(dst, std::max<size_t>(bytes, 16)));
@@ -470,6 +493,7 @@ static int32_t upload_impl(sq_ctx* ctx, int32_t dim, int32_t narrow, uint32_t n_
   if (b->n_wide) {
     if ((rc = up((void**)&b->d_wnodes, wnodes.data(), wnodes.size() * 4))) return cleanup(rc);
     if ((rc = up((void**)&b->d_wsrc, wsrc.data(), wsrc.size() * 4))) return cleanup(rc);
+    if (!qnodes.empty() && (rc = up((void**)&b->d_qnodes, qnodes.data(), qnodes.size() * 4))) return cleanup(rc);
   }
   if ((rc = up((void**)&b->d_prims, prims.data(), prims.size() * 4))) return cleanup(rc);
   if ((rc = up((void**)&b->d_root, node_bounds, size_t(2) * D * 4))) return cleanup(rc);
@@ -522,7 +546,7 @@ extern "C" int32_t sq_bvh_destroy(sq_bvh* b) {
   cudaSetDevice(b->device);
   void* ptrs[] = {b->d_nodes, b->d_prims, b->d_root, b->d_layers, b->d_sub, b->d_prim_ids,
                   b->d_leaves, b->d_parents, b->d_arrivals, b->d_refit_in, b->d_nonfinite,
-                  b->d_nb64, b->d_nc64, b->d_prims64, b->d_wnodes, b->d_wsrc};
+                  b->d_nb64, b->d_nc64, b->d_prims64, b->d_wnodes, b->d_wsrc, b->d_qnodes};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete b;
@@ -575,6 +599,14 @@ extern "C" int32_t sq_bvh_refit_d(sq_ctx* ctx, sq_bvh* b, const float* d_prim_da
     void* wargs[] = {&wn, &bn, &src, &slots};
     CK(cudaLaunchKernel(b->ks.wide_sync, dim3((slots + 255) / 256), dim3(256), wargs, 0, ctx->stream));
     ctx->launches++;
+    if (b->d_qnodes && b->ks.quant_sync) {
+      float4* qn = b->d_qnodes;
+      const float4* wsrc4 = b->d_wnodes;
+      uint32_t recs = b->n_wide;
+      void* qargs[] = {&qn, &wsrc4, &recs};
+      CK(cudaLaunchKernel(b->ks.quant_sync, dim3((recs + 127) / 128), dim3(128), qargs, 0, ctx->stream));
+      ctx->launches++;
+    }
   }
   return finish(ctx);
 }
@@ -1359,17 +1391,19 @@ extern "C" int32_t sq_autotune_nearest_d(sq_ctx* ctx, const sq_bvh* b, const flo
   o.leaf = d_leaf;
   o.toi = d_toi;
   const int saved_order = ctx->order, saved_bps = ctx->blocks_per_sm, saved_layout = ctx->layout;
-  // (order, layout): near-first over child-pair records, near-first over
-  // four-wide records (when the scene has them), the reference order.
-  const int orders[3] = {SQ_ORDER_NEAR_FIRST, SQ_ORDER_NEAR_FIRST, SQ_ORDER_REFERENCE};
-  const int layouts[3] = {SQ_LAYOUT_BINARY, SQ_LAYOUT_WIDE, SQ_LAYOUT_BINARY};
+  // (order, layout): near-first over child-pair records, over four-wide
+  // records and over quantised four-wide records (when the scene has them),
+  // the reference order.
+  const int orders[4] = {SQ_ORDER_NEAR_FIRST, SQ_ORDER_NEAR_FIRST, SQ_ORDER_NEAR_FIRST, SQ_ORDER_REFERENCE};
+  const int layouts[4] = {SQ_LAYOUT_BINARY, SQ_LAYOUT_WIDE, SQ_LAYOUT_QUANT, SQ_LAYOUT_BINARY};
   const int bps[8] = {0, 2, 4, 6, 8, 10, 12, 16};
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   float best = 0.f;
-  for (int oi = 0; oi < 3 && rc == SQ_OK; ++oi) {
+  for (int oi = 0; oi < 4 && rc == SQ_OK; ++oi) {
     if (layouts[oi] == SQ_LAYOUT_WIDE && !(b->n_wide && b->ks.ray_nearest_wide)) continue;
+    if (layouts[oi] == SQ_LAYOUT_QUANT && !(b->n_wide && b->d_qnodes && b->ks.ray_nearest_quant)) continue;
     for (int bi = 0; bi < 8 && rc == SQ_OK; ++bi) {
       ctx->order = orders[oi];
       ctx->layout = layouts[oi];

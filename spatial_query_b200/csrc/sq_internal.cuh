@@ -86,6 +86,8 @@ struct sq_bvh {
   float4* d_wnodes = nullptr;
   uint32_t* d_wsrc = nullptr;
   uint32_t n_wide = 0, wroot = 0, wdepth = 0;
+  // The same four-wide records quantised (QuantLayout), same numbering.
+  float4* d_qnodes = nullptr;
   // An f64 scene (sq_bvh_upload_f64): node boxes, node links and leaf
   // parameters in double, answered only by the _f64 entry points.
   int prec = 32;
@@ -190,6 +192,7 @@ inline uint32_t prim_vec(int dim, int narrow) {
 
 inline uint32_t node_vec(int dim) { return (4 * dim + 2 + 3) / 4; }
 inline uint32_t wide_vec(int dim) { return (8 * dim + 4 + 3) / 4; }
+inline uint32_t quant_vec(int dim) { return (dim + (dim + 3) / 4 + 2 * dim + 4 + 3) / 4; }
 
 inline int32_t arena_reserve(sq_ctx* ctx, size_t bytes) {
   if (ctx->arena.cap >= bytes) return SQ_OK;

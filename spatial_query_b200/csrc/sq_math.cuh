@@ -27,7 +27,7 @@ constexpr uint32_t kNoHit = 0xFFFFFFFFu;
 constexpr uint32_t kLeafBit = 0x80000000u;
 
 // Per-scalar constants: EPSILON (f32 / f64) and the triangle test's two
-// literals (viewport-lib-query/src/lib.rs:295-320), in the scalar's precision.
+// literals (viewport-lib-query/src/lib.rs:281-306), in the scalar's precision.
 template <class S> struct Lim;
 template <> struct Lim<float> {
   static constexpr float eps = 1.1920928955078125e-7f;  // f32::EPSILON
@@ -143,10 +143,10 @@ __device__ __forceinline__ bool slab_fast(const RayPre<D>& r, const float* lo, c
 
 // The same slab against a box grown by a probe: ShapeCast::broadphase
 // (query/shapecast.rs:70-73): grown = [lo - probe.max, hi - probe.min].
-template <int D>
-__device__ __forceinline__ bool slab_grown(const RayPre<D>& r, const float* lo, const float* hi, const float* pmin,
-                                           const float* pmax, float max_toi, float& t_enter, int& axis) {
-  float glo[D], ghi[D];
+template <int D, class S>
+__device__ __forceinline__ bool slab_grown(const RayPre<D, S>& r, const S* lo, const S* hi, const S* pmin,
+                                           const S* pmax, S max_toi, S& t_enter, int& axis) {
+  S glo[D], ghi[D];
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     glo[i] = fsub(lo[i], pmax[i]);
@@ -237,7 +237,7 @@ __device__ __forceinline__ bool ray_ball(const S* o, const S* d, const S* c, S r
 }
 
 // glam Vec3 dot / cross, the operations of the reference triangle test
-// (crates/viewport-lib-query/src/lib.rs:295-320).
+// (crates/viewport-lib-query/src/lib.rs:281-306).
 template <class S> __device__ __forceinline__ S gdot(const S* a, const S* b) {
   return fadd(fadd(fmul(a[0], b[0]), fmul(a[1], b[1])), fmul(a[2], b[2]));
 }
@@ -287,6 +287,14 @@ __device__ __forceinline__ void tri_aabb(const float* v0, const float* v1, const
   for (int i = 0; i < 3; ++i) {
     lo[i] = fminf(fminf(fminf(__int_as_float(0x7f800000), v0[i]), v1[i]), v2[i]);
     hi[i] = fmaxf(fmaxf(fmaxf(__int_as_float(0xff800000), v0[i]), v1[i]), v2[i]);
+  }
+}
+__device__ __forceinline__ void tri_aabb(const double* v0, const double* v1, const double* v2, double* lo,
+                                         double* hi) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    lo[i] = fmin(fmin(fmin(__longlong_as_double(0x7ff0000000000000ll), v0[i]), v1[i]), v2[i]);
+    hi[i] = fmax(fmax(fmax(__longlong_as_double(0xfff0000000000000ll), v0[i]), v1[i]), v2[i]);
   }
 }
 

@@ -650,11 +650,15 @@ __global__ void __launch_bounds__(kThreads, (IK == kInstMesh && !REF && !STATS) 
     }
   };
 
-  // Mesh instances, nearest rays: a lane walks its instances' BLASes inside
-  // the same descent loop as the top level, one leaf per pass, so that lanes
-  // in different levels and instances share the node-test instructions
-  // instead of each lane finishing a whole BLAS walk (blas_nearest) while
-  // the rest of its warp waits. Same visits, same order, same answers.
+  // Mesh instances, rays (nearest, all hits, crossings): a lane walks its
+  // instances' BLASes inside the same descent loop as the top level, one
+  // leaf per pass, so that lanes in different levels and instances share
+  // the node-test instructions instead of each lane finishing a whole BLAS
+  // walk (blas_nearest) while the rest of its warp waits. Same visits, same
+  // order, same answers: nearest rays walk a BLAS near-first with the
+  // certificate, list rays walk it in the crate's own order (their
+  // instance hits are never answered again, so they need none) and list the
+  // instance's hit.
   bool in_blas = false;
   bool b_last = false;    // the instance is the last of its top-level leaf
   uint32_t b_pos = 0;     // instance record whose BLAS is walked
@@ -664,7 +668,7 @@ __global__ void __launch_bounds__(kThreads, (IK == kInstMesh && !REF && !STATS) 
   float b_limit = 0.f, b_cut = 0.f, b_t = 0.f;
   uint32_t b_best = kNoHit, b_flag = 0u;
   float b_n[3] = {0.f, 0.f, 0.f};
-  auto unified = [&]() { return IK == kInstMesh && L.kind == kTRayNearest; };
+  auto unified = [&]() { return IK == kInstMesh && L.kind <= kTRayCross; };
 
   // blas_nearest's box test and leaf, on the lane's BLAS state.
   auto btest = [&](const float* lo, const float* hi, float& te) -> bool {
@@ -687,7 +691,7 @@ __global__ void __launch_bounds__(kThreads, (IK == kInstMesh && !REF && !STATS) 
           b_t = t;
           b_limit = t;
           b_cut = t;
-          if (!REF && !L.ref) {
+          if (!REF && !L.ref && L.kind == kTRayNearest) {
             // certify the new best: not before its own triangle's AABB entry
             float lo[3], hi[3], te;
             int ax;

@@ -71,6 +71,108 @@ template <int D> struct WideLayout {
   static constexpr int vec = (words + 3) / 4;
 };
 
+// Quantised four-wide records: the same four-wide tree (same numbering and
+// codes), each child's box stored as 8-bit steps from the record's origin
+// (the lower corner of the union of its children) in a power-of-two step per
+// axis, rounded outward: a stored box always contains the exact one, so its
+// slab entry is never later and the walk never prunes a subtree the exact
+// boxes would keep (it may visit a few more; answers are certified as for
+// every near-first walk). Words: origin[D] (f32), the D step exponents
+// (biased by 127, one byte each), the 8 x D step counts (child k, axis i: lo
+// at byte 2Dk + i, hi at byte 2Dk + D + i), then the four codes.
+template <int D> struct QuantLayout {
+  static constexpr int exp_words = (D + 3) / 4;
+  static constexpr int o_exp = D;
+  static constexpr int o_q = D + exp_words;
+  static constexpr int o_code = D + exp_words + 2 * D;
+  static constexpr int words = o_code + 4;
+  static constexpr int vec = (words + 3) / 4;
+};
+
+// origin + q x 2^e, in the arithmetic both the quantiser and the walk use.
+__host__ __device__ __forceinline__ float q_decode(float origin, uint32_t q, float step) {
+#ifdef __CUDA_ARCH__
+  return __fadd_rn(origin, __fmul_rn(float(q), step));
+#else
+  volatile float m = float(q) * step;  // exact: q < 256 and step a power of two
+  return origin + m;
+#endif
+}
+
+__host__ __device__ __forceinline__ float q_step(uint32_t biased) {
+  union { uint32_t u; float f; } v;
+  v.u = biased << 23;
+  return v.f;
+}
+
+__host__ __device__ __forceinline__ uint32_t q_byte(const uint32_t* words, int index) {
+  return (words[index >> 2] >> (8 * (index & 3))) & 0xFFu;
+}
+
+// Quantises one four-wide record: lo/hi of child k at box + 2Dk, codes[k]
+// (kNoHit: an empty slot). Writes QuantLayout<D>::words words. Non-finite
+// bounds give a record of zeros (the walk reads the exact records of a scene
+// with non-finite bounds).
+template <int D>
+__host__ __device__ void quantize_record(const float* box, const uint32_t* codes, uint32_t* out) {
+  using QL = QuantLayout<D>;
+  for (int w = 0; w < QL::words; ++w) out[w] = 0u;
+  for (int k = 0; k < 4; ++k) out[QL::o_code + k] = codes[k];
+  float plo[D], phi[D];
+  bool finite = true, any = false;
+  for (int i = 0; i < D; ++i) {
+    plo[i] = 3.4028235e38f;
+    phi[i] = -3.4028235e38f;
+  }
+  for (int k = 0; k < 4; ++k) {
+    if (codes[k] == kNoHit) continue;
+    any = true;
+    for (int i = 0; i < D; ++i) {
+      const float lo = box[2 * D * k + i], hi = box[2 * D * k + D + i];
+      finite = finite && (lo - lo == 0.f) && (hi - hi == 0.f);  // false for inf and NaN
+      plo[i] = lo < plo[i] ? lo : plo[i];
+      phi[i] = hi > phi[i] ? hi : phi[i];
+    }
+  }
+  if (!finite || !any) return;
+  union { float f; uint32_t u; } cv;
+  for (int i = 0; i < D; ++i) {
+    cv.f = plo[i];
+    out[i] = cv.u;
+    // the smallest step whose 255th multiple reaches the upper corner
+    uint32_t e = 1;  // biased exponent 1..254
+    const float ext = phi[i] - plo[i];
+    if (ext > 0.f) {
+      cv.f = ext;
+      const int ex = int((cv.u >> 23) & 0xFFu) - 127;  // ext in [2^ex, 2^(ex+1)) for normal ext
+      int b = ex - 7 + 127;  // 255 x 2^(ex-7) < 2^(ex+1): start just below
+      b = b < 1 ? 1 : (b > 254 ? 254 : b);
+      e = uint32_t(b);
+      while (e < 254 && q_decode(plo[i], 255u, q_step(e)) < phi[i]) ++e;
+      while (e > 1 && q_decode(plo[i], 255u, q_step(e - 1)) >= phi[i]) --e;
+    }
+    out[QL::o_exp + (i >> 2)] |= e << (8 * (i & 3));
+    const float step = q_step(e);
+    for (int k = 0; k < 4; ++k) {
+      if (codes[k] == kNoHit) continue;
+      const float lo = box[2 * D * k + i], hi = box[2 * D * k + D + i];
+      // lo: the largest q whose decoded value is <= lo (q = 0 decodes to the origin <= lo)
+      float fq = (lo - plo[i]) / step;
+      uint32_t ql = fq <= 0.f ? 0u : (fq >= 255.f ? 255u : uint32_t(fq));
+      while (ql > 0 && q_decode(plo[i], ql, step) > lo) --ql;
+      while (ql < 255 && q_decode(plo[i], ql + 1, step) <= lo) ++ql;
+      // hi: the smallest q whose decoded value is >= hi (q = 255 reaches the upper corner)
+      fq = (hi - plo[i]) / step;
+      uint32_t qh = fq <= 0.f ? 0u : (fq >= 255.f ? 255u : uint32_t(fq));
+      while (qh < 255 && q_decode(plo[i], qh, step) < hi) ++qh;
+      while (qh > ql && q_decode(plo[i], qh - 1, step) >= hi) --qh;
+      const int bl = 2 * D * k + i, bh = 2 * D * k + D + i;
+      out[QL::o_q + (bl >> 2)] |= ql << (8 * (bl & 3));
+      out[QL::o_q + (bh >> 2)] |= qh << (8 * (bh & 3));
+    }
+  }
+}
+
 template <int D, int N> struct PrimLayout {
   static constexpr int payload = (N == kNarrowAabb)     ? 2 * D
                                  : (N == kNarrowTri)    ? 9
@@ -87,6 +189,7 @@ template <int K> struct QueryLayout {
 struct QueryParams {
   const float4* __restrict__ nodes;
   const float4* __restrict__ wnodes;  // four-wide records (WIDE kernels)
+  const float4* __restrict__ qnodes;  // quantised four-wide records (QUANT kernels; same numbering)
   uint32_t wroot;                     // the root's four-wide code
   const float4* __restrict__ prims;
   const uint64_t* __restrict__ layers;
@@ -324,6 +427,7 @@ template <int D, int K> struct Lane {
   uint32_t best_pos; // near-first: primitive position of the best hit (for its certification)
   uint32_t q;
   uint32_t code;
+  float code_t;      // entry of the node in code (postponed-leaf walks re-check it after a leaf)
   int sp;
   bool fast;
   uint32_t best_leaf;
@@ -351,9 +455,10 @@ template <int D, int K> struct Lane {
 // WIDE (near-first nearest rays, no counters, no seed): the walk reads the
 // four-wide records; a step tests up to four children, goes to the nearest
 // and stacks the others farthest first.
-template <int D, int N, int K, bool REF, bool STATS, bool SEED = false, bool WIDE = false>
+template <int D, int N, int K, bool REF, bool STATS, bool SEED = false, bool WIDE = false, bool QUANT = false>
 __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   static_assert(!WIDE || (K == kRayNearest && !REF && !STATS && !SEED), "four-wide walks serve near-first rays only");
+  static_assert(!QUANT || WIDE, "quantised records are a four-wide layout");
   constexpr bool kNearest = (K == kRayNearest || K == kCastNearest);
   constexpr bool kCast = (K == kCastNearest || K == kCastAll);
   constexpr bool kList = (K == kRayAll || K == kCastAll);
@@ -378,6 +483,10 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   const uint32_t n_queries = p.q_count ? *p.q_count : p.n;
 
   constexpr bool DETECT = kNearest && !REF;
+  // Postponed leaves for the certified near-first walks (their answers do
+  // not depend on the order of the visits); the counting and reference-order
+  // walks keep the crate's sequence.
+  constexpr bool SPEC = DETECT && !STATS && !WIDE;
   const float kInf = __int_as_float(0x7f800000);
 
   // Box test of one child (or the root) against the lane's query: the slab
@@ -407,6 +516,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
       --L.sp;
       L.code = s_code[L.sp * kThreads + tid];
       const float t = s_t[L.sp * kThreads + tid];
+      L.code_t = t;
       if (!kNearest || t <= L.limit) return true;
     }
     return false;
@@ -509,6 +619,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
     }
     float te;
     const bool hit_root = test_box(lo, hi, te);
+    L.code_t = te;
     if constexpr (SEED) {
       const int32_t bk = p.seed_bucket[q];
       if (hit_root && bk >= 0 && uint32_t(bk) < p.n_buckets) {
@@ -553,6 +664,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
               }
             }
             L.code = e.x;
+            L.code_t = tb;
           }
         }
       }
@@ -561,8 +673,8 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   };
 
   // Tests the primitives of the leaf in L.code.
-  auto leaf = [&]() {
-    uint32_t pos = L.code & ~kLeafBit;
+  auto leaf = [&](uint32_t code) {
+    uint32_t pos = code & ~kLeafBit;
     for (;;) {
       float rec[PL::vec * 4];
       load_vec<PL::vec>(p.prims + size_t(pos) * PL::vec, rec);
@@ -693,24 +805,111 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
       if (__all_sync(FULL, exhausted)) break;
       continue;
     }
-    if (live) {
+    if constexpr (SPEC) {
+      if (live) {
+        // Postponed leaves (Aila and Laine's speculative traversal): a lane
+        // that reaches a leaf holds it and keeps descending from the next
+        // waiting node until every live lane of the warp holds a leaf or
+        // has nothing left, so the leaf tests below run with the warp
+        // together. The extra nodes are visited with the limit as it stood,
+        // which only adds work: near-first answers are certified whatever
+        // the order of the visits.
+        uint32_t pend = kNoHit;
+        bool empty = false;  // nothing left to walk after pend
+        for (;;) {
+          if (!empty) {
+            if (L.code & kLeafBit) {
+              if (pend == kNoHit) {
+                pend = L.code;
+                if (!pop()) empty = true;
+              }
+            } else {
+              float rec[NL::vec * 4];
+              load_vec<NL::vec>(p.nodes + size_t(L.code) * NL::vec, rec);
+              const uint32_t ca = __float_as_uint(rec[4 * D]);
+              const uint32_t cb = __float_as_uint(rec[4 * D + 1]);
+              float ta, tb;
+              const bool pa = test_box(rec, rec + D, ta);
+              const bool pb = test_box(rec + 2 * D, rec + 3 * D, tb);
+              if (pa && pb) {
+                const bool a_first = ta <= tb;
+                s_code[L.sp * kThreads + tid] = a_first ? cb : ca;
+                s_t[L.sp * kThreads + tid] = a_first ? tb : ta;
+                ++L.sp;
+                L.code = a_first ? ca : cb;
+                L.code_t = a_first ? ta : tb;
+              } else if (pa) {
+                L.code = ca;
+                L.code_t = ta;
+              } else if (pb) {
+                L.code = cb;
+                L.code_t = tb;
+              } else if (!pop()) {
+                empty = true;
+              }
+            }
+          }
+          if (__all_sync(live_mask, pend != kNoHit || empty)) break;
+        }
+        if (pend != kNoHit) leaf(pend);
+        // The node after the leaf was taken with the limit as it stood:
+        // drop it (and what follows, as pop does) if the leaf's hit prunes it.
+        if (!empty && L.code_t > L.limit && !pop()) empty = true;
+        if (empty) {
+          live = false;
+          finish();
+        }
+      }
+    } else if (live) {
       bool done = false;
       // Descend interior records until a leaf comes up.
       while (!(L.code & kLeafBit)) {
         if constexpr (WIDE) {
-          float rec[WL::vec * 4];
-          load_vec<WL::vec>(p.wnodes + size_t(L.code) * WL::vec, rec);
           float t4[4];
           uint32_t c4[4];
+          bool exact = true;
+          if constexpr (QUANT) {
+            if (scene_finite) {
+              // Decode each child's box (rounded outward) and test it.
+              using QL = QuantLayout<D>;
+              float qf[QL::vec * 4];
+              load_vec<QL::vec>(p.qnodes + size_t(L.code) * QL::vec, qf);
+              uint32_t qw[QL::vec * 4];
 #pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            c4[i] = __float_as_uint(rec[8 * D + i]);
-            float te = kInf;
-            if (c4[i] == kNoHit || !test_box(rec + 2 * D * i, rec + 2 * D * i + D, te)) {
-              c4[i] = kNoHit;
-              te = kInf;
+              for (int w = 0; w < QL::vec * 4; ++w) qw[w] = __float_as_uint(qf[w]);
+#pragma unroll
+              for (int k = 0; k < 4; ++k) {
+                c4[k] = qw[QL::o_code + k];
+                float lo[D], hi[D];
+#pragma unroll
+                for (int i = 0; i < D; ++i) {
+                  const float step = q_step(q_byte(qw + QL::o_exp, i));
+                  lo[i] = q_decode(qf[i], q_byte(qw + QL::o_q, 2 * D * k + i), step);
+                  hi[i] = q_decode(qf[i], q_byte(qw + QL::o_q, 2 * D * k + D + i), step);
+                }
+                float te = kInf;
+                if (c4[k] == kNoHit || !test_box(lo, hi, te)) {
+                  c4[k] = kNoHit;
+                  te = kInf;
+                }
+                t4[k] = te;
+              }
+              exact = false;
             }
-            t4[i] = te;
+          }
+          if (exact) {
+            float rec[WL::vec * 4];
+            load_vec<WL::vec>(p.wnodes + size_t(L.code) * WL::vec, rec);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              c4[i] = __float_as_uint(rec[8 * D + i]);
+              float te = kInf;
+              if (c4[i] == kNoHit || !test_box(rec + 2 * D * i, rec + 2 * D * i + D, te)) {
+                c4[i] = kNoHit;
+                te = kInf;
+              }
+              t4[i] = te;
+            }
           }
           // Ascending entry order (a five-comparator network); misses sort last.
           auto cswap = [&](int a, int b) {
@@ -780,7 +979,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
         }
       }
       if (!done) {
-        leaf();
+        leaf(L.code);
         done = !pop();
       }
       if (done) {
@@ -1011,6 +1210,26 @@ template <int D, int N> __global__ void __launch_bounds__(256) refit_kernel(cons
   }
 }
 
+// After a refit (and wide_sync_kernel): every quantised record is quantised
+// again from its exact four-wide record.
+template <int D>
+__global__ void quant_sync_kernel(float4* qnodes, const float4* __restrict__ wnodes, uint32_t n_records) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_records) return;
+  float rec[WideLayout<D>::vec * 4];
+  load_vec<WideLayout<D>::vec>(wnodes + size_t(r) * WideLayout<D>::vec, rec);
+  uint32_t codes[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) codes[k] = __float_as_uint(rec[8 * D + k]);
+  uint32_t out[QuantLayout<D>::vec * 4];
+#pragma unroll
+  for (int w = 0; w < QuantLayout<D>::vec * 4; ++w) out[w] = 0u;
+  quantize_record<D>(rec, codes, out);
+  uint4* dst = reinterpret_cast<uint4*>(qnodes + size_t(r) * QuantLayout<D>::vec);
+#pragma unroll
+  for (int w = 0; w < QuantLayout<D>::vec; ++w) dst[w] = make_uint4(out[4 * w], out[4 * w + 1], out[4 * w + 2], out[4 * w + 3]);
+}
+
 // Function-pointer table entry for one (D, narrow) pair.
 // After a refit: every four-wide slot copies its box from the binary record
 // slot that holds the same node's box (src = record << 1 | slot).
@@ -1028,7 +1247,9 @@ __global__ void wide_sync_kernel(float4* wnodes, const float4* __restrict__ node
 struct KernelSet {
   const void* ray_nearest[2][2];  // [ref][stats]
   const void* ray_nearest_wide;   // near-first over the four-wide records
+  const void* ray_nearest_quant;  // near-first over the quantised four-wide records
   const void* wide_sync;          // refreshes four-wide boxes from the binary records
+  const void* quant_sync;         // quantises the four-wide records again
   const void* ray_all[2];         // [stats]
   const void* cast_nearest[2];    // [ref]
   const void* cast_all;
@@ -1046,7 +1267,9 @@ template <int D, int N> KernelSet make_kernel_set() {
   s.ray_nearest[1][0] = (const void*)query_kernel<D, N, kRayNearest, true, false>;
   s.ray_nearest[1][1] = (const void*)query_kernel<D, N, kRayNearest, true, true>;
   s.ray_nearest_wide = (const void*)query_kernel<D, N, kRayNearest, false, false, false, true>;
+  s.ray_nearest_quant = (const void*)query_kernel<D, N, kRayNearest, false, false, false, true, true>;
   s.wide_sync = (const void*)wide_sync_kernel<D>;
+  s.quant_sync = (const void*)quant_sync_kernel<D>;
   s.ray_all[0] = (const void*)query_kernel<D, N, kRayAll, true, false>;
   s.ray_all[1] = (const void*)query_kernel<D, N, kRayAll, true, true>;
   s.cast_nearest[0] = (const void*)query_kernel<D, N, kCastNearest, false, false>;

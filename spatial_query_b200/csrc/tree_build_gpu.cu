@@ -19,6 +19,13 @@
 // left), and leaves every other position where it is. Nodes are numbered in
 // level order as they are made; preorder numbers follow from subtree sizes
 // (bottom-up, a level at a time) and left-subtree offsets (top-down).
+//
+// The host never waits inside the build: a median split halves the longest
+// segment, so the number of levels and a bound on each level's segment count
+// follow from n alone; grids are sized by those bounds and every kernel reads
+// the level's true segment count from device memory (a one-thread kernel
+// closes each level). The one synchronisation is at the end, for the node
+// count the call returns.
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
@@ -70,7 +77,7 @@ struct LevelParams {
   const uint32_t* keys;  // [D][n]
   const uint32_t* idx;   // the current primitive order
   const Seg* cur;
-  uint32_t m;            // segments of this level
+  const uint32_t* m;     // segments of this level (device memory)
   Seg* next;             // the next level's segments (appended)
   uint32_t* counters;    // [0] next segments, [1] nodes made, [2] split segments
   LNode* nodes;          // by level-order id
@@ -123,6 +130,16 @@ __device__ int decide(const LevelParams& p, const Seg& sg, const float* lo, cons
   return axis;
 }
 
+// Closes level L: the next level's segments were appended with level-order
+// ids [made - count, made); records them and clears the per-level counters.
+__global__ void advance_kernel(uint32_t* counters, uint32_t* level_info, uint32_t L) {
+  const uint32_t m_next = counters[0], made = counters[1];
+  level_info[2 * (L + 1)] = made - m_next;
+  level_info[2 * (L + 1) + 1] = m_next;
+  counters[0] = 0;
+  counters[2] = 0;
+}
+
 // Every position keeps its place unless a split segment claims it.
 __global__ void place_keys_kernel(unsigned long long* sort_keys, uint32_t n) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -141,6 +158,7 @@ __global__ void red_init_kernel(uint32_t* red, uint32_t m) {
 // of segment g and folds its result into the segment's bounds.
 __global__ void __launch_bounds__(256) red_kernel(const LevelParams p) {
   const uint32_t g = blockIdx.y;
+  if (g >= *p.m) return;  // the grid covers the level's bound
   const Seg sg = p.cur[g];
   const uint64_t b0 = uint64_t(sg.s) + uint64_t(blockIdx.x) * p.chunk;
   if (b0 >= sg.e) return;  // uniform per block
@@ -191,7 +209,7 @@ __global__ void __launch_bounds__(256) red_kernel(const LevelParams p) {
 // Top levels: leaf or split per segment from the reduced bounds.
 __global__ void decide_kernel(const LevelParams p) {
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= p.m) return;
+  if (g >= *p.m) return;
   const uint32_t* r = p.red + size_t(g) * 4 * kMaxDim;
   float lo[kMaxDim], hi[kMaxDim], clo[kMaxDim], chi[kMaxDim];
   for (int k = 0; k < p.D; ++k) {
@@ -206,6 +224,7 @@ __global__ void decide_kernel(const LevelParams p) {
 // Top levels: the sort keys of the split segments' positions, chunked like red_kernel.
 __global__ void split_keys_kernel(const LevelParams p) {
   const uint32_t g = blockIdx.y;
+  if (g >= *p.m) return;
   const int axis = p.axis[g];
   if (axis < 0) return;
   const Seg sg = p.cur[g];
@@ -224,7 +243,7 @@ __global__ void __launch_bounds__(256) level_kernel(const LevelParams p) {
   const uint32_t groups = blockDim.x / TPS;
   const uint32_t g = blockIdx.x * groups + threadIdx.x / TPS;
   const uint32_t lane = threadIdx.x % TPS;
-  if (g >= p.m) return;  // uniform per warp
+  if (g >= *p.m) return;  // uniform per warp
   const int D = p.D;
   const Seg sg = p.cur[g];
   float lo[kMaxDim], hi[kMaxDim], clo[kMaxDim], chi[kMaxDim];
@@ -269,20 +288,23 @@ __global__ void __launch_bounds__(256) level_kernel(const LevelParams p) {
     p.sort_keys[pos] = ((unsigned long long)sg.s << 32) | key[p.idx[pos]];
 }
 
-// Subtree node counts, one level at a time from the deepest.
-__global__ void sizes_kernel(const LNode* __restrict__ nodes, uint32_t lb, uint32_t le, uint32_t* size) {
-  const uint32_t id = lb + blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= le) return;
+// Subtree node counts, one level at a time from the deepest (level L's ids
+// are [level_info[2L], + level_info[2L + 1])).
+__global__ void sizes_kernel(const LNode* __restrict__ nodes, const uint32_t* level_info, uint32_t L, uint32_t* size) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= level_info[2 * L + 1]) return;
+  const uint32_t id = level_info[2 * L] + i;
   const LNode nd = nodes[id];
   size[id] = nd.a == kNone ? 1u : 1u + size[nd.a] + size[nd.b];
 }
 
 // Preorder numbers, one level at a time from the root: the left child
 // follows its parent, the right child follows the left subtree.
-__global__ void preorder_kernel(const LNode* __restrict__ nodes, uint32_t lb, uint32_t le, const uint32_t* size,
-                                uint32_t* pre) {
-  const uint32_t id = lb + blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= le) return;
+__global__ void preorder_kernel(const LNode* __restrict__ nodes, const uint32_t* level_info, uint32_t L,
+                                const uint32_t* size, uint32_t* pre) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= level_info[2 * L + 1]) return;
+  const uint32_t id = level_info[2 * L] + i;
   const LNode nd = nodes[id];
   if (nd.a == kNone) return;
   pre[nd.a] = pre[id] + 1;
@@ -292,10 +314,10 @@ __global__ void preorder_kernel(const LNode* __restrict__ nodes, uint32_t lb, ui
 // The crate's node arrays in preorder (tree::Node: bounds, and either the
 // children's indices or the leaf's first position and count).
 __global__ void emit_kernel(const LNode* __restrict__ nodes, const float* __restrict__ lbounds,
-                            const uint32_t* __restrict__ pre, uint32_t n_nodes, int D, float* node_bounds,
-                            uint32_t* child_a, uint32_t* child_b, uint32_t* prim_count) {
+                            const uint32_t* __restrict__ pre, const uint32_t* made, uint32_t capacity, int D,
+                            float* node_bounds, uint32_t* child_a, uint32_t* child_b, uint32_t* prim_count) {
   const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= n_nodes) return;
+  if (id >= *made || id >= capacity) return;
   const LNode nd = nodes[id];
   const uint32_t i = pre[id];
   for (int k = 0; k < 2 * D; ++k) node_bounds[size_t(i) * 2 * D + k] = lbounds[size_t(id) * 2 * D + k];
@@ -332,15 +354,32 @@ extern "C" int32_t sq_tree_build_d(sq_ctx* ctx, int32_t dim, uint32_t n, const f
   const int D = dim;
   const size_t N2 = size_t(2) * n;  // node capacity of the level-order arrays
 
+  // The levels: a median split halves the longest segment, and a segment of
+  // at most kLeafSize primitives is a leaf, so the level where the longest
+  // segment first fits a leaf is the last; level L has at most min(2^L, n)
+  // segments.
+  std::vector<uint64_t> longest_at{n};
+  while (longest_at.back() > kLeafSize) longest_at.push_back((longest_at.back() + 1) / 2);
+  const uint32_t n_levels = uint32_t(longest_at.size());
+  auto bound_at = [&](uint32_t L) { return L >= 32 ? uint64_t(n) : std::min<uint64_t>(uint64_t(1) << L, n); };
+
   // Scratch, carved from one stream-ordered allocation.
   sqi::Carve cv;
   constexpr uint32_t kWide = 1024;  // levels with this many segments or more: one warp per segment
+  size_t sort_bytes = 0;
+  int pos_bits = 1;
+  while (pos_bits < 32 && (uint64_t(1) << pos_bits) < n) ++pos_bits;
+  const int end_bit = 32 + pos_bits;  // positions fit in the keys' high word
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, static_cast<unsigned long long*>(nullptr),
+                                     static_cast<unsigned long long*>(nullptr), static_cast<uint32_t*>(nullptr),
+                                     static_cast<uint32_t*>(nullptr), int(n), 0, end_bit, st));
   const size_t o_keys = cv.take(size_t(D) * n * 4), o_idx0 = cv.take(size_t(n) * 4), o_idx1 = cv.take(size_t(n) * 4),
                o_sk0 = cv.take(size_t(n) * 8), o_sk1 = cv.take(size_t(n) * 8),
                o_seg0 = cv.take((size_t(n) + 1) * sizeof(Seg)), o_seg1 = cv.take((size_t(n) + 1) * sizeof(Seg)),
                o_red = cv.take(size_t(kWide) * 4 * kMaxDim * 4), o_axis = cv.take(size_t(kWide) * 4),
                o_nodes = cv.take(N2 * sizeof(LNode)), o_lb = cv.take(N2 * 2 * D * 4), o_size = cv.take(N2 * 4),
-               o_pre = cv.take(N2 * 4), o_ctr = cv.take(16);
+               o_pre = cv.take(N2 * 4), o_ctr = cv.take(16), o_lv = cv.take(size_t(2) * (n_levels + 1) * 4),
+               o_sort = cv.take(sort_bytes);
   char* base = nullptr;
   CK(cudaMallocAsync(reinterpret_cast<void**>(&base), cv.off, st));
   uint32_t* keys = reinterpret_cast<uint32_t*>(base + o_keys);
@@ -357,11 +396,9 @@ extern "C" int32_t sq_tree_build_d(sq_ctx* ctx, int32_t dim, uint32_t n, const f
   uint32_t* size = reinterpret_cast<uint32_t*>(base + o_size);
   uint32_t* pre = reinterpret_cast<uint32_t*>(base + o_pre);
   uint32_t* ctr = reinterpret_cast<uint32_t*>(base + o_ctr);
-  void* temp = nullptr;
-  size_t temp_cap = 0;
-  int32_t rc = SQ_OK;
+  uint32_t* level_info = reinterpret_cast<uint32_t*>(base + o_lv);
+  void* temp = base + o_sort;
   auto done = [&](int32_t code) {
-    if (temp) cudaFreeAsync(temp, st);
     cudaFreeAsync(base, st);
     return code;
   };
@@ -375,71 +412,54 @@ extern "C" int32_t sq_tree_build_d(sq_ctx* ctx, int32_t dim, uint32_t n, const f
   CKB(cudaGetLastError());
   const Seg root{0, n, 0};
   CKB(cudaMemcpyAsync(cur, &root, sizeof(Seg), cudaMemcpyHostToDevice, st));
-  const uint32_t init[4] = {0, 1, 0, 0};
+  const uint32_t init[4] = {0, 1, 0, 0};  // next segments, nodes made, split segments
   CKB(cudaMemcpyAsync(ctr, init, sizeof(init), cudaMemcpyHostToDevice, st));
-  std::vector<std::pair<uint32_t, uint32_t>> levels;  // level-order id ranges
-  // Positions fit in the keys' high word: a stable sort over bits
-  // [0, 32 + pos_bits) orders by (segment start, key).
-  int pos_bits = 1;
-  while (pos_bits < 32 && (uint64_t(1) << pos_bits) < n) ++pos_bits;
-  const int end_bit = 32 + pos_bits;
-  uint32_t m = 1, made = 1;
+  const uint32_t root_level[2] = {0, 1};  // level 0: id 0, one segment
+  CKB(cudaMemcpyAsync(level_info, root_level, sizeof(root_level), cudaMemcpyHostToDevice, st));
   uint64_t own_launches = 1;  // keys_kernel
-  uint64_t longest = n;  // bound on this level's longest segment (median splits halve it)
-  while (m > 0) {
-    levels.emplace_back(made - m, made);
-    CKB(cudaMemsetAsync(ctr, 0, 4, st));      // next segments
-    CKB(cudaMemsetAsync(ctr + 2, 0, 4, st));  // split segments
-    place_keys_kernel<<<std::min<uint32_t>(blocks_for(n, 256), 148 * 8), 256, 0, st>>>(skeys, n);
-    LevelParams p{d_prim_aabbs, D, n, keys, idx, cur, m, nxt, ctr, nodes, lbounds, skeys, red, axis, 4096u};
-    own_launches += m >= kWide ? 2 : 5;
-    if (m >= kWide) {
-      level_kernel<32><<<blocks_for(m, 8), 256, 0, st>>>(p);
+  for (uint32_t L = 0; L < n_levels; ++L) {
+    const uint64_t bound = bound_at(L), longest = longest_at[L];
+    const bool may_split = longest > kLeafSize;  // false only on the last level
+    if (may_split) place_keys_kernel<<<std::min<uint32_t>(blocks_for(n, 256), 148 * 8), 256, 0, st>>>(skeys, n);
+    LevelParams p{d_prim_aabbs, D, n, keys, idx, cur, level_info + 2 * L + 1, nxt, ctr, nodes, lbounds, skeys, red,
+                  axis, 4096u};
+    if (bound >= kWide) {
+      level_kernel<32><<<blocks_for(bound, 8), 256, 0, st>>>(p);
+      own_launches += 1;
     } else {
-      const dim3 grid(uint32_t(std::max<uint64_t>(1, (longest + p.chunk - 1) / p.chunk)), m);
-      red_init_kernel<<<blocks_for(uint64_t(m) * 4 * kMaxDim, 256), 256, 0, st>>>(red, m);
+      const dim3 grid(uint32_t(std::max<uint64_t>(1, (longest + p.chunk - 1) / p.chunk)), uint32_t(bound));
+      red_init_kernel<<<blocks_for(bound * 4 * kMaxDim, 256), 256, 0, st>>>(red, uint32_t(bound));
       red_kernel<<<grid, 256, 0, st>>>(p);
-      decide_kernel<<<blocks_for(m, 128), 128, 0, st>>>(p);
+      decide_kernel<<<blocks_for(bound, 128), 128, 0, st>>>(p);
       split_keys_kernel<<<grid, 256, 0, st>>>(p);
+      own_launches += 4;
     }
+    advance_kernel<<<1, 1, 0, st>>>(ctr, level_info, L);
+    own_launches += 1 + (may_split ? 1 : 0);
     CKB(cudaGetLastError());
-    uint32_t h[4];
-    CKB(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st));
-    CKB(cudaStreamSynchronize(st));
-    const uint32_t n_next = h[0], n_split = h[2];
-    made = h[1];
-    if (n_split > 0) {
-      size_t need = 0;
-      CKB(cub::DeviceRadixSort::SortPairs(nullptr, need, skeys, skeys_alt, idx, idx_alt, int(n), 0, end_bit, st));
-      if (need > temp_cap) {
-        if (temp) CKB(cudaFreeAsync(temp, st));
-        temp = nullptr;
-        temp_cap = 0;
-        CKB(cudaMallocAsync(&temp, need, st));
-        temp_cap = need;
-      }
+    if (may_split) {
+      size_t need = sort_bytes;
       CKB(cub::DeviceRadixSort::SortPairs(temp, need, skeys, skeys_alt, idx, idx_alt, int(n), 0, end_bit, st));
       std::swap(idx, idx_alt);
+      own_launches += 1;
     }
     std::swap(cur, nxt);
-    m = n_next;
-    longest = (longest + 1) / 2;
   }
-  const uint32_t n_nodes = made;
-  if (n_nodes > node_capacity) return done(fail(ctx, SQ_ERR_CAPACITY, "node_capacity too small"));
-  for (size_t L = levels.size(); L-- > 0;) {
-    const auto [lb, le] = levels[L];
-    sizes_kernel<<<blocks_for(le - lb, 256), 256, 0, st>>>(nodes, lb, le, size);
-  }
+  for (uint32_t L = n_levels; L-- > 0;)
+    sizes_kernel<<<blocks_for(bound_at(L), 256), 256, 0, st>>>(nodes, level_info, L, size);
   CKB(cudaMemsetAsync(pre, 0, 4, st));
-  for (const auto& [lb, le] : levels) preorder_kernel<<<blocks_for(le - lb, 256), 256, 0, st>>>(nodes, lb, le, size, pre);
-  emit_kernel<<<blocks_for(n_nodes, 256), 256, 0, st>>>(nodes, lbounds, pre, n_nodes, D, d_node_bounds, d_child_a,
-                                                        d_child_b, d_prim_count);
+  for (uint32_t L = 0; L < n_levels; ++L)
+    preorder_kernel<<<blocks_for(bound_at(L), 256), 256, 0, st>>>(nodes, level_info, L, size, pre);
+  emit_kernel<<<blocks_for(uint64_t(2) * n - 1, 256), 256, 0, st>>>(nodes, lbounds, pre, ctr + 1, node_capacity, D,
+                                                                    d_node_bounds, d_child_a, d_child_b, d_prim_count);
   CKB(cudaGetLastError());
   CKB(cudaMemcpyAsync(d_prim_indices, idx, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
-  ctx->launches += own_launches + 2 * levels.size() + 1;
-  rc = done(SQ_OK);
+  uint32_t n_nodes = 0;
+  CKB(cudaMemcpyAsync(&n_nodes, ctr + 1, 4, cudaMemcpyDeviceToHost, st));
+  ctx->launches += own_launches + 2 * n_levels + 1;
+  int32_t rc = done(SQ_OK);
   CK(cudaStreamSynchronize(st));
+  if (n_nodes > node_capacity) return fail(ctx, SQ_ERR_CAPACITY, "node_capacity too small");
   *n_nodes_out = n_nodes;
 #undef CKB
   return rc;

@@ -121,3 +121,141 @@ def test_f32_and_f64_scenes_stay_apart(ctx):
     assert rc == sq.SQ_ERR_UNSUPPORTED
     s64.close()
     s32.close()
+
+
+# -- lists, casts and overlap with Scalar = f64 ---------------------------------
+
+def scene64(ctx, geom):
+    return sq.DeviceBvh64(ctx, sq.HostBvh.build_f64(geom.dim, geom.world_aabbs_f64()), geom)
+
+
+def same_lists64(ref, got, label):
+    assert np.array_equal(ref.count, got.count), f"{label}: counts differ on {(ref.count != got.count).sum()}"
+    k = ref.leaf.shape[1]
+    mask = np.arange(k)[None, :] < np.minimum(ref.count, k)[:, None]
+    assert np.array_equal(ref.leaf[mask], got.leaf[mask]), f"{label}: list leaves"
+    assert np.array_equal(ref.toi[mask].view(np.uint64), got.toi[mask].view(np.uint64)), f"{label}: f64 list toi"
+    assert np.array_equal(ref.normal[mask].view(np.uint32), got.normal[mask].astype(np.float32).view(np.uint32)), \
+        f"{label}: list normals"
+
+
+def same_nearest64(ref, got, label):
+    assert np.array_equal(ref.leaf, got.leaf), f"{label}: leaf differs on {(ref.leaf != got.leaf).sum()}"
+    assert np.array_equal(ref.toi.view(np.uint64), got.toi.view(np.uint64)), f"{label}: f64 toi"
+    assert np.array_equal(ref.normal.view(np.uint32), got.normal.astype(np.float32).view(np.uint32)), \
+        f"{label}: normals"
+
+
+def box_casts(rng, n, dim, lo, hi, hlo, hhi):
+    o = rng.range(lo, hi, (n, dim))
+    d = scenes.normalize_rows(rng.range(-1.0, 1.0, (n, dim)))
+    h = rng.range(hlo, hhi, (n, dim))
+    return np.ascontiguousarray(np.concatenate([o, d, -h, h], axis=1), dtype=np.float32)
+
+
+def regions(rng, n, dim, lo, hi, hlo, hhi):
+    c = rng.range(lo, hi, (n, dim))
+    h = rng.range(hlo, hhi, (n, dim))
+    return np.ascontiguousarray(np.concatenate([c - h, c + h], axis=1), dtype=np.float32)
+
+
+@pytest.mark.parametrize("dim", [2, 3, 6])
+def test_lists_casts_overlap_boxes(ctx, dim):
+    s = scenes.boxes_scene(seed=70 + dim, n_boxes=8000, n_rays=4096, dim=dim)
+    prims = s["prims"]
+    if dim >= 4:
+        c, h = (prims[:, :dim] + prims[:, dim:]) / 2, (prims[:, dim:] - prims[:, :dim]) / 2
+        prims = np.ascontiguousarray(np.concatenate([c - 6 * h, c + 6 * h], axis=1), dtype=np.float32)
+    geom = sq.Geometry("boxes", dim, prims)
+    o = O.Scene("boxes", dim, prims, prec=64)
+    g = scene64(ctx, geom)
+    rng = scenes.Rng(80 + dim)
+    rays = s["rays"]
+    ra = o.all(rays, s["max_toi"], k=16)
+    assert (ra.count > 1).sum() > 50
+    same_lists64(ra, g.raycast_all(rays.astype(np.float64), s["max_toi"], k=16), f"all D={dim}")
+    casts = box_casts(rng, 4096, dim, -120.0, 120.0, 0.2, 3.0)
+    lens = rng.range(0.0, 300.0, 4096).astype(np.float32)
+    cn = o.shapecast_nearest(casts, lens)
+    assert (cn.leaf != O.NO_HIT).sum() > 50
+    same_nearest64(cn, g.shapecast_nearest(casts.astype(np.float64), lens.astype(np.float64)), f"cast D={dim}")
+    same_lists64(o.shapecast_all(casts, lens, k=8), g.shapecast_all(casts.astype(np.float64), lens.astype(np.float64),
+                                                                      k=8), f"cast all D={dim}")
+    reg = regions(rng, 4096, dim, -100.0, 100.0, 0.5, 12.0)
+    want = o.overlap(reg)
+    assert want[1].size > 100
+    got = g.overlap(reg.astype(np.float64))
+    assert np.array_equal(want[0], got[0]) and np.array_equal(want[1], got[1]), f"overlap D={dim}"
+    g.close()
+
+
+@pytest.mark.parametrize("kind", ["balls", "balls_near"])
+def test_crossings_casts_overlap_balls(ctx, kind):
+    rng = scenes.Rng(90)
+    n = 6000
+    prims = np.concatenate([rng.range(-60.0, 60.0, (n, 3)), rng.range(0.3, 3.0, (n, 1))], axis=1).astype(np.float32)
+    o0 = rng.range(-100.0, 100.0, (4096, 3))
+    d = scenes.normalize_rows(rng.range(-50.0, 50.0, (4096, 3)) - o0)
+    rays = np.ascontiguousarray(np.concatenate([o0, d], axis=1), dtype=np.float32)
+    geom = sq.Geometry(kind, 3, prims)
+    o = O.Scene(kind, 3, prims, prec=64)
+    g = scene64(ctx, geom)
+    cr = o.all(rays, 400.0, k=24, crossings=True)
+    assert (cr.count >= 2).sum() > 100
+    same_lists64(cr, g.raycast_crossings(rays.astype(np.float64), 400.0, k=24), f"{kind} crossings")
+    same_lists64(o.all(rays, 400.0, k=24), g.raycast_all(rays.astype(np.float64), 400.0, k=24), f"{kind} all")
+    # ball casts: the probe's max[0] is the swept radius
+    casts = box_casts(rng, 4096, 3, -80.0, 80.0, 0.5, 0.5)
+    cn = o.shapecast_nearest(casts, 200.0)
+    assert (cn.leaf != O.NO_HIT).sum() > 100
+    same_nearest64(cn, g.shapecast_nearest(casts.astype(np.float64), 200.0), f"{kind} cast")
+    reg = regions(rng, 4096, 3, -60.0, 60.0, 0.5, 8.0)
+    want = o.overlap(reg)
+    got = g.overlap(reg.astype(np.float64))
+    assert np.array_equal(want[0], got[0]) and np.array_equal(want[1], got[1]), f"{kind} overlap"
+    g.close()
+
+
+def test_triangles_lists_casts_overlap_filter(ctx):
+    s = scenes.terrain_scene(seed=8, nx=96, ny=64, n_coherent=4096, n_incoherent=4096)
+    layers = (np.arange(s["prims"].shape[0]) % 3 + 1).astype(np.uint64)
+    geom = sq.Geometry("tris", 3, s["prims"], layers=layers)
+    o = O.Scene("tris", 3, s["prims"], layers=layers, prec=64)
+    g = scene64(ctx, geom)
+    rng = scenes.Rng(91)
+    rays = s["rays"]
+    same_lists64(o.all(rays, s["max_toi"], k=16), g.raycast_all(rays.astype(np.float64), s["max_toi"], k=16),
+                 "tri all")
+    same_lists64(o.all(rays, s["max_toi"], k=16, mask=0b10), g.raycast_all(rays.astype(np.float64), s["max_toi"],
+                                                                            k=16, mask=0b10), "tri all filtered")
+    lo, hi = s["prims"].reshape(-1, 3).min(axis=0), s["prims"].reshape(-1, 3).max(axis=0)
+    o0 = rng.range(0.0, 1.0, (4096, 3)) * (hi - lo) + lo
+    o0[:, 2] = hi[2] + 5.0
+    d = scenes.normalize_rows(np.concatenate([rng.range(-0.3, 0.3, (4096, 2)), -np.ones((4096, 1))], axis=1))
+    h = rng.range(0.2, 2.0, (4096, 3))
+    casts = np.ascontiguousarray(np.concatenate([o0, d, -h, h], axis=1), dtype=np.float32)
+    cn = o.shapecast_nearest(casts, 500.0)
+    assert (cn.leaf != O.NO_HIT).mean() > 0.5
+    same_nearest64(cn, g.shapecast_nearest(casts.astype(np.float64), 500.0), "tri cast")
+    same_lists64(o.shapecast_all(casts, 500.0, k=8), g.shapecast_all(casts.astype(np.float64), 500.0, k=8),
+                 "tri cast all")
+    c = rng.range(0.0, 1.0, (2048, 3)) * (hi - lo) + lo
+    hh = rng.range(0.5, 6.0, (2048, 3))
+    reg = np.ascontiguousarray(np.concatenate([c - hh, c + hh], axis=1), dtype=np.float32)
+    want = o.overlap(reg, mask=0b101)
+    got = g.overlap(reg.astype(np.float64), mask=0b101)
+    assert want[1].size > 100
+    assert np.array_equal(want[0], got[0]) and np.array_equal(want[1], got[1]), "tri overlap filtered"
+    g.close()
+
+
+def test_f64_lists_empty_scene_and_no_queries(ctx):
+    geom = sq.Geometry("boxes", 3, np.zeros((0, 6), np.float32))
+    g = scene64(ctx, geom)
+    r = g.raycast_all(np.array([[0, 0, 0, 1, 0, 0]], np.float64), 10.0, k=4)
+    assert r.count[0] == 0
+    off, lv = g.overlap(np.array([[-1, -1, -1, 1, 1, 1]], np.float64))
+    assert list(off) == [0, 0] and lv.size == 0
+    c = g.shapecast_nearest(np.zeros((0, 12), np.float64), 10.0)
+    assert c.leaf.size == 0
+    g.close()

@@ -186,6 +186,8 @@ def test_mesh_instances_small(small_instanced, order):
     assert_same_nearest(ref, g.raycast_nearest(s["rays"], s["max_toi"]), label="mesh nearest")
     assert_same_lists(o.all(s["rays"], s["max_toi"], k=8), g.raycast_all(s["rays"], s["max_toi"], k=8),
                       label="mesh all")
+    assert_same_lists(o.all(s["rays"], s["max_toi"], k=8, crossings=True),
+                      g.raycast_crossings(s["rays"], s["max_toi"], k=8), label="mesh crossings")
     assert_same_nearest(o.shapecast_nearest(s["casts"], s["cast_len"]),
                         g.shapecast_nearest(s["casts"], s["cast_len"]), label="mesh casts")
     assert_same_csr(o.overlap(s["regions"]), g.overlap(s["regions"]), label="mesh overlaps")
