@@ -838,8 +838,8 @@ def main():
                        "identical_hits": identical,
                        "plain_gpu": {"value": round(plain_value, 3), "unit": "Mrays/s", "ms_per_step": round(plain_ms, 4),
                                      "path": "plain GPU traversal, autotuned: "
-                                             + (("near-first, " + ("four-wide" if tune["best"]["layout"] == 1
-                                                                   else "child-pair") + " records")
+                                             + (("near-first, " + {1: "four-wide", 2: "quantised four-wide"}.get(
+                                                 tune["best"]["layout"], "child-pair") + " records")
                                                 if tune["best"]["order"] == 0 else "reference order")
                                              + f", {tune['best']['blocks_per_sm'] or 'occupancy'} blocks per SM",
                                      "e2e_mrays": round(world * n / (e2e_plain_ms / 1000) / 1e6, 3),
@@ -851,6 +851,9 @@ def main():
                                     "four_wide_best_ms": round(min((e["ms"] for e in tune["table"]
                                                                     if e["order"] == 0 and e["layout"] == 1),
                                                                    default=float("nan")), 4),
+                                    "quantised_four_wide_best_ms": round(min((e["ms"] for e in tune["table"]
+                                                                              if e["order"] == 0 and e["layout"] == 2),
+                                                                             default=float("nan")), 4),
                                     "reference_best_ms": round(min(e["ms"] for e in tune["table"] if e["order"] == 1), 4)},
                        "all_hits_k16": {"value": round(world * n / (all_ms / 1000) / 1e6, 3), "unit": "Mrays/s",
                                         "ms_per_step": round(all_ms, 4),

@@ -516,7 +516,7 @@ class DeviceBvh:
         self.tree = tree
 
     def autotune_nearest_d(self, d_rays, n, max_toi, reps: int = 3) -> dict:
-        """Times the order x blocks-per-SM candidates on these rays, keeps the
+        """Times the order x layout x blocks-per-SM candidates on these rays, keeps the
         fastest in the context (sq_autotune_nearest_d); returns the table."""
         r = _TuneResult()
         self.ctx.check(lib().sq_autotune_nearest_d(self.ctx.h, self.h, _p(d_rays), n, float(max_toi), reps,

@@ -1,5 +1,5 @@
 """The nearest-ray autotuner (sq_autotune_nearest_d): it times every order x
-blocks-per-SM candidate, keeps the fastest in the context, and the tuned
+node-layout x blocks-per-SM candidate, keeps the fastest in the context, and the tuned
 context still returns the oracle's hits bit for bit."""
 import numpy as np
 import pytest
@@ -22,8 +22,9 @@ def test_autotune_keeps_hits_exact():
     d_rays = torch.from_numpy(s["rays"]).to(torch.device("cuda", 0))
     torch.cuda.synchronize()
     res = scene.autotune_nearest_d(d_rays, n, s["max_toi"], reps=2)
-    assert len(res["table"]) == 24  # near-first binary, near-first four-wide, reference: 8 grids each
-    assert {(e["order"], e["layout"]) for e in res["table"]} == {(0, 0), (0, 1), (1, 0)}
+    # near-first over child-pair, four-wide and quantised four-wide records, the reference order: 8 grids each
+    assert len(res["table"]) == 32
+    assert {(e["order"], e["layout"]) for e in res["table"]} == {(0, 0), (0, 1), (0, 2), (1, 0)}
     assert all(e["ms"] > 0 for e in res["table"])
     assert res["best"]["ms"] == min(e["ms"] for e in res["table"])
     ref = O.Scene("tris", 3, s["prims"]).nearest(s["rays"], s["max_toi"])
