@@ -783,6 +783,37 @@ def main():
     e2e_plain_ms = e2e_time(e2e_plain)
     e2e_value = world * n / (e2e_ms / 1000) / 1e6
 
+    # The guide where a tight early limit is worth more: the crate's own
+    # far-first child order. Plain reference order against the seeded walk
+    # in the same order (trained predictions, and every ray's true bucket);
+    # all answers identical.
+    ctx.set_order(sq.ORDER_REFERENCE)
+    st_r = scene.raycast_nearest_d(d_rays, n, s["max_toi"], d_leaf, d_toi, d_nrm, stats=True)
+    st_rt = guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], g_leaf, g_toi, g_nrm, d_bucket=d_bucket,
+                                           stats=True)
+    torch.cuda.synchronize()
+    same_r = bool(torch.equal(g_leaf, d_leaf) and torch.equal(g_toi.view(torch.int32), d_toi.view(torch.int32)))
+    st_rp = guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], p_leaf, p_toi, p_nrm, d_bucket=d_lt, stats=True)
+    torch.cuda.synchronize()
+    same_r = same_r and bool(torch.equal(p_leaf, d_leaf) and torch.equal(p_toi.view(torch.int32),
+                                                                          d_toi.view(torch.int32)))
+    if not same_r:
+        raise SystemExit("far-first seeded hits differ from the plain query's")
+    r_plain_ms = mean_max(timed(stream, plain, args.steps, flush))
+    r_seed_ms = mean_max(timed(stream, seeded, args.steps, flush))
+    r_perfect_ms = mean_max(timed(stream, perfect, args.steps, flush))
+    r_guided_ms = mean_max(timed(stream, guided, args.steps, flush))
+    ctx.set_order(tune["best"]["order"])
+    far_first = {"what": "the crate's child order (push a, push b) after the seed, certified; plain = the reference "
+                         "order", "identical_hits": same_r,
+                 "plain": {"ms": round(r_plain_ms, 4), "nodes_visited_per_ray": round(st_r["nodes_visited"] / n, 3)},
+                 "seeded_trained": {"ms": round(r_seed_ms, 4),
+                                    "nodes_visited_per_ray": round(st_rt["nodes_visited"] / n, 3)},
+                 "seeded_true_bucket": {"ms": round(r_perfect_ms, 4),
+                                        "nodes_visited_per_ray": round(st_rp["nodes_visited"] / n, 3)},
+                 "learned_seeded_ms": round(r_guided_ms, 4),
+                 "learned_vs_plain": round(r_plain_ms / r_guided_ms, 4)}
+
     peak, peak_kind = measured_peaks()
     tpeak = tensor_peak()
     mlp_flop = 2 * MLP_MACS * n
@@ -870,6 +901,7 @@ def main():
                                         "narrow_tests_per_ray": round(st_p["narrow_tests"] / n, 3),
                                         "seeded_traversal_ms": round(perfect_ms, 4),
                                         "plain_traversal_ms": round(plain_ms, 4)},
+                       "guide_far_first_order": far_first,
                        "learned_vs_plain_bound": {
                            "mlp_ms_at_peak": round(mlp_flop / (tpeak[0] * 1e12) * 1000, 4),
                            "plain_ms": round(plain_ms, 4),

@@ -96,7 +96,10 @@ int32_t sq_guide_predict_d(sq_guide* g, const float* d_rays, uint32_t n, int32_t
  * predicted and walked on the context's stream and on its internal second
  * lane (own stream and scratch, joined back to the context's stream before
  * the call returns); the first such call of a batch size sizes that lane's
- * scratch, so it belongs outside a stream capture. */
+ * scratch, so it belongs outside a stream capture. After the predicted
+ * bucket the walk follows the context's order (sq_ctx_set_order): near-first,
+ * or the crate's child order (push a, push b); either way each answer is
+ * certified and equals the reference's. */
 int32_t sq_raycast_nearest_guided_d(sq_ctx* ctx, const sq_bvh* bvh, const sq_guide* g, const float* d_rays,
                                     uint32_t n, float max_toi, const int32_t* d_bucket, const sq_hits* out,
                                     sq_query_stats* stats);

@@ -1225,6 +1225,10 @@ int32_t sqi::seeded_nearest(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, u
     p.bucket_sibs = seeds.sibs;
     p.n_buckets = seeds.n_buckets;
     p.sib_stride = seeds.sib_stride;
+    // The walk after the bucket follows the context's order: near-first, or
+    // the crate's own child order (still certified: the seed changes the
+    // visiting order, so the crate's counters are not replayed).
+    p.far_first = ctx->order == SQ_ORDER_REFERENCE ? 1 : 0;
     if (st) p.stats = ctx->d_stats;
     // The bucket's ancestors' other children wait on the stack (one per level
     // above the bucket) while the bucket is searched: no deeper than a plain

@@ -228,6 +228,7 @@ struct QueryParams {
   uint32_t k;
   int crossings;
   int fill;  // overlap: 0 count, 1 fill in ascending order, 2 fill in walk order
+  int far_first;  // seeded walks: after the bucket, the crate's child order (push a, push b) instead of near-first
   // Overlap regions that visit more than visit_budget records in the count
   // pass are left to overlap_heavy_kernel (a warp per region): listed in
   // heavy_list, flagged in heavy_flag (the fill pass skips them).
@@ -832,7 +833,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
               const bool pa = test_box(rec, rec + D, ta);
               const bool pb = test_box(rec + 2 * D, rec + 3 * D, tb);
               if (pa && pb) {
-                const bool a_first = ta <= tb;
+                const bool a_first = (SEED && p.far_first) ? false : (ta <= tb);
                 s_code[L.sp * kThreads + tid] = a_first ? cb : ca;
                 s_t[L.sp * kThreads + tid] = a_first ? tb : ta;
                 ++L.sp;
@@ -964,7 +965,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
         if (pa && pb) {
           // Reference order: child_a waits, child_b goes first. Near-first:
           // the smaller entry goes first.
-          const bool a_first = (REF || !kNearest) ? false : (ta <= tb);
+          const bool a_first = (REF || !kNearest || (SEED && p.far_first)) ? false : (ta <= tb);
           s_code[L.sp * kThreads + tid] = a_first ? cb : ca;
           s_t[L.sp * kThreads + tid] = a_first ? tb : ta;
           ++L.sp;

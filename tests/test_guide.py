@@ -154,16 +154,20 @@ def test_seeded_hits_identical_whatever_the_seed(ctx, terrain):
         "random": torch.randint(0, info["n_buckets"], (n,), generator=gen, dtype=torch.int32).to(DEV),
         "out_of_range": torch.randint(-5, info["n_buckets"] + 5, (n,), generator=gen, dtype=torch.int32).to(DEV),
     }
-    for name, d_b in seeds.items():
-        leaf = torch.empty(n, dtype=torch.int32, device=DEV)
-        toi = torch.empty(n, dtype=torch.float32, device=DEV)
-        nrm = torch.empty((n, 3), dtype=torch.float32, device=DEV)
-        torch.cuda.synchronize()
-        guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], leaf, toi, nrm, d_bucket=d_b)
-        ctx.synchronize()
-        assert torch.equal(leaf, leaf0), name
-        assert torch.equal(toi.view(torch.int32), toi0.view(torch.int32)), name
-        assert torch.equal(nrm.view(torch.int32), nrm0.view(torch.int32)), name
+    # after the seed the walk follows the context's order: near-first, or the crate's far-first child order
+    for order in (sq.ORDER_NEAR_FIRST, sq.ORDER_REFERENCE):
+        ctx.set_order(order)
+        for name, d_b in seeds.items():
+            leaf = torch.empty(n, dtype=torch.int32, device=DEV)
+            toi = torch.empty(n, dtype=torch.float32, device=DEV)
+            nrm = torch.empty((n, 3), dtype=torch.float32, device=DEV)
+            torch.cuda.synchronize()
+            guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], leaf, toi, nrm, d_bucket=d_b)
+            ctx.synchronize()
+            assert torch.equal(leaf, leaf0), (order, name)
+            assert torch.equal(toi.view(torch.int32), toi0.view(torch.int32)), (order, name)
+            assert torch.equal(nrm.view(torch.int32), nrm0.view(torch.int32)), (order, name)
+    ctx.set_order(sq.ORDER_NEAR_FIRST)
     # and the host-buffer entry point against the CPU oracle on a slice
     o = O.Scene("tris", 3, s["prims"])
     sl = s["rays"][:65536]
