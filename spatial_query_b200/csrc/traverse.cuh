@@ -55,6 +55,18 @@ __device__ void sq_narrow_crossings(const float* prim, uint32_t leaf, const floa
 enum QKind : int { kRayNearest = 0, kRayAll = 1, kCastNearest = 2, kCastAll = 3, kOverlap = 4 };
 
 constexpr int kThreads = 128;
+
+// The certified near-first walks keep the top entry of each lane's stack in
+// registers; older entries spill to the shared-memory stack ([depth][thread]).
+// The child pushed last is the one popped first whenever the near child's
+// subtree ends in a leaf, so that pop costs no shared-memory round trip.
+#ifndef SQ_REG_TOP
+#define SQ_REG_TOP 1
+#endif
+// Postponed leaves in the certified near-first walks (see query_kernel).
+#ifndef SQ_POSTPONE_LEAVES
+#define SQ_POSTPONE_LEAVES 1
+#endif
 constexpr int kMaxStack = 96;  // deepest tree accepted (96 KB of stack per block)
 
 template <int D> struct NodeLayout {
@@ -429,6 +441,9 @@ template <int D, int K> struct Lane {
   uint32_t q;
   uint32_t code;
   float code_t;      // entry of the node in code (postponed-leaf walks re-check it after a leaf)
+  uint32_t top_code; // postponed-leaf walks: the stack's top entry, held in registers
+  float top_t;
+  bool has_top;
   int sp;
   bool fast;
   uint32_t best_leaf;
@@ -487,7 +502,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   // Postponed leaves for the certified near-first walks (their answers do
   // not depend on the order of the visits); the counting and reference-order
   // walks keep the crate's sequence.
-  constexpr bool SPEC = DETECT && !STATS && !WIDE;
+  constexpr bool SPEC = SQ_POSTPONE_LEAVES && DETECT && !STATS && !WIDE;
   const float kInf = __int_as_float(0x7f800000);
 
   // Box test of one child (or the root) against the lane's query: the slab
@@ -513,6 +528,14 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   // Pops the next waiting child whose entry still lies within the limit
   // (exactly the reference's slab verdict at pop time). False: stack empty.
   auto pop = [&]() -> bool {
+    if constexpr (SPEC && SQ_REG_TOP) {
+      if (L.has_top) {
+        L.has_top = false;
+        L.code = L.top_code;
+        L.code_t = L.top_t;
+        if (L.top_t <= L.limit) return true;
+      }
+    }
     while (L.sp > 0) {
       --L.sp;
       L.code = s_code[L.sp * kThreads + tid];
@@ -611,6 +634,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
     L.v_nar = 0;
     L.v_hit = 0;
     L.sp = 0;
+    L.has_top = false;
     L.code = WIDE ? p.wroot : p.root_code;
     float lo[D], hi[D];
 #pragma unroll
@@ -834,9 +858,22 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
               const bool pb = test_box(rec + 2 * D, rec + 3 * D, tb);
               if (pa && pb) {
                 const bool a_first = (SEED && p.far_first) ? false : (ta <= tb);
-                s_code[L.sp * kThreads + tid] = a_first ? cb : ca;
-                s_t[L.sp * kThreads + tid] = a_first ? tb : ta;
-                ++L.sp;
+                const uint32_t far_code = a_first ? cb : ca;
+                const float far_t = a_first ? tb : ta;
+                if (SQ_REG_TOP) {
+                  if (L.has_top) {  // the register entry spills below the new one
+                    s_code[L.sp * kThreads + tid] = L.top_code;
+                    s_t[L.sp * kThreads + tid] = L.top_t;
+                    ++L.sp;
+                  }
+                  L.top_code = far_code;
+                  L.top_t = far_t;
+                  L.has_top = true;
+                } else {
+                  s_code[L.sp * kThreads + tid] = far_code;
+                  s_t[L.sp * kThreads + tid] = far_t;
+                  ++L.sp;
+                }
                 L.code = a_first ? ca : cb;
                 L.code_t = a_first ? ta : tb;
               } else if (pa) {
