@@ -301,7 +301,10 @@ __global__ void __launch_bounds__(128) walk64_kernel(const Params64 p) {
           if (cast64<D, N>(rec, r, pmin, pmax, limit, t, nrm)) put64<D>(p, q, count, t, id, nrm);
         } else {  // kRayAll
           bool listed = false;
-          if constexpr (N == kNarrowSphere || N == kNarrowSphereNear) {
+          // Both roots for the ball whose test reports the far root from
+          // inside (tests/crossings.rs:505-521); the near-root-only ball lists
+          // one crossing per hit, as the f32 kernels do.
+          if constexpr (N == kNarrowSphere) {
             if (p.crossings) {
               // Both roots of the unbounded ray (tests/crossings.rs:505-521).
               listed = true;
