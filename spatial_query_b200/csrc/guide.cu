@@ -565,274 +565,6 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
 }
 
 // ---------------------------------------------------------------------------
-// Fused inference with the activations in tensor memory.
-//
-// The output layer is 32 jobs of M = 128 rays x N = 128 buckets x K = 128
-// per half-tile. With both operands in shared memory every K = 16 step
-// reads 4 KB of A and 4 KB of B for 64 cycles of tensor work, which is the
-// SM's shared-memory bandwidth; here each hidden layer's bf16 output is
-// written by the epilogue into tensor memory and read from there as the A
-// operand (the TS form of tcgen05.mma), so only the weight chunk streams from
-// shared memory. Tensor memory (512 columns): the two halves' activations
-// (64 columns each: 128 bf16 per row, two per column), then three 128-column
-// accumulators that the jobs of both halves take in turn (job K of a tile
-// sequence uses accumulator K mod 3, half K mod 2), so the epilogue of a job
-// has two jobs of tensor work to finish before its accumulator is reused.
-// ---------------------------------------------------------------------------
-constexpr int kRingTs = 4;
-
-struct InferTsSmem {
-  static constexpr uint32_t feat = 0;                           // 2 halves x 16 KB (layer-1 operand, K = 16 used)
-  static constexpr uint32_t w1 = 32768;                         // 16 KB
-  static constexpr uint32_t ring = w1 + 16384;                  // 4 x 32 KB
-  static constexpr uint32_t bias = ring + kRingTs * kChunkBytes;  // (384 + 4096) floats max
-  static constexpr uint32_t bars = bias + (384 + 4096) * 4;
-  static constexpr uint32_t bytes = bars + 256 + 1024;
-};
-
-__global__ void __launch_bounds__(kInferThreads, 1) guide_infer_ts_kernel(const InferParams p) {
-  extern __shared__ uint8_t smem_raw[];
-  const uint32_t raw = umma::smem_u32(smem_raw);
-  uint8_t* base = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base + InferTsSmem::bars);
-  uint64_t* w_full = bars + 0;
-  uint64_t* ring_full = bars + 1;                // [4]
-  uint64_t* ring_empty = bars + 1 + kRingTs;     // [4]
-  uint64_t* acc_full = bars + 1 + 2 * kRingTs;   // [3]
-  uint64_t* acc_empty = bars + 4 + 2 * kRingTs;  // [3]
-  uint64_t* act_ready = bars + 7 + 2 * kRingTs;  // [half]
-  uint64_t* fin = bars + 9 + 2 * kRingTs;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 10 + 2 * kRingTs);
-  int* s_err = reinterpret_cast<int*>(bars + 11 + 2 * kRingTs);
-  uint32_t* s_r7f = reinterpret_cast<uint32_t*>(bars + 12 + 2 * kRingTs);  // 0x7F, for tag7
-  const float* s_bias = reinterpret_cast<const float*>(base + InferTsSmem::bias);
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t n_tiles = (p.n + 255) / 256;
-  const uint32_t bias_bytes = (384 + p.n_chunks * 128) * 4;
-  const uint32_t jobs = 3 + p.n_chunks;  // per half and tile: three hidden layers, then the output chunks
-  constexpr uint32_t idesc = umma::idesc_bf16(128, 128);
-  constexpr uint32_t kAccCol = 128;  // accumulators start after the two halves' activations
-
-  if (threadIdx.x == 0) {
-    umma::mbar_init(w_full, 1);
-    for (int s = 0; s < kRingTs; ++s) {
-      umma::mbar_init(&ring_full[s], 1);
-      umma::mbar_init(&ring_empty[s], 1);
-    }
-    for (int k = 0; k < 3; ++k) {
-      umma::mbar_init(&acc_full[k], 1);
-      umma::mbar_init(&acc_empty[k], 4);
-    }
-    umma::mbar_init(&act_ready[0], 4);
-    umma::mbar_init(&act_ready[1], 4);
-    umma::mbar_init(fin, 1);
-    *s_err = 0;
-    *s_r7f = 0x7Fu;
-    umma::fence_barrier_init();
-  }
-  __syncwarp();
-  if (warp == 1) umma::tmem_alloc(tslot, 512);
-  umma::tc_fence_before();
-  __syncthreads();
-  umma::tc_fence_after();
-  const uint32_t tbase = *tslot;
-  auto failed = [&]() { return *(volatile int*)s_err != 0; };
-  auto set_err = [&](int code) { atomicCAS(s_err, 0, code); };
-
-  if (warp == 0) {
-    if (lane == 0) {
-      // Producer: W1 + biases once, then per tile W2, W3 and the W4 chunks.
-      umma::mbar_arrive_expect_tx(w_full, 16384 + bias_bytes);
-      umma::bulk_load(base + InferTsSmem::w1, p.w1_img, 16384, w_full);
-      umma::bulk_load(base + InferTsSmem::bias, p.bias, bias_bytes, w_full);
-      uint32_t G = 0;
-      for (uint32_t t = blockIdx.x; t < n_tiles && !failed(); t += gridDim.x) {
-        for (uint32_t j = 0; j < 2 + p.n_chunks; ++j, ++G) {
-          const uint32_t slot = G % kRingTs;
-          if (G >= kRingTs && !umma::mbar_wait(&ring_empty[slot], ((G / kRingTs) + 1) & 1)) {
-            set_err(1);
-            break;
-          }
-          const uint8_t* src = j < 2 ? p.w23_img + size_t(j) * kChunkBytes : p.w4_img + size_t(j - 2) * kChunkBytes;
-          umma::mbar_arrive_expect_tx(&ring_full[slot], kChunkBytes);
-          umma::bulk_load(base + InferTsSmem::ring + slot * kChunkBytes, src, kChunkBytes, &ring_full[slot]);
-        }
-      }
-      // Let every copy issued land before shared memory is released.
-      for (uint32_t k = (G > kRingTs ? G - kRingTs : 0); k < G; ++k)
-        umma::mbar_wait(&ring_full[k % kRingTs], (k / kRingTs) & 1, 100000000ull);
-      umma::mbar_wait(w_full, 0, 100000000ull);
-    }
-  } else if (warp == 1) {
-    if (lane == 0) {
-      // MMA issuer: job K (both halves, in order) accumulates into K mod 3.
-      if (!umma::mbar_wait(w_full, 0)) set_err(2);
-      uint32_t G = 0, K = 0, A[2] = {0u, 0u};
-      const uint32_t w1d = umma::smem_u32(base + InferTsSmem::w1);
-      bool ok = true;
-      for (uint32_t t = blockIdx.x; ok && t < n_tiles && !failed(); t += gridDim.x) {
-        for (uint32_t j = 0; ok && j < jobs && !failed(); ++j) {
-          uint32_t slot = 0;
-          if (j >= 1) {
-            slot = G % kRingTs;
-            if (!umma::mbar_wait(&ring_full[slot], (G / kRingTs) & 1)) { set_err(5); break; }
-          }
-          for (uint32_t h = 0; h < 2; ++h, ++K) {
-            const uint32_t b = K % 3, u = K / 3;
-            // Layer 1 waits for the features, layers 2-4 for the previous layer's activations.
-            if (j <= 3) {
-              if (!umma::mbar_wait(&act_ready[h], A[h] & 1)) { set_err(3); ok = false; break; }
-              ++A[h];
-            }
-            if (u >= 1 && !umma::mbar_wait(&acc_empty[b], (u - 1) & 1)) {
-              set_err(4);
-              ok = false;
-              break;
-            }
-            umma::tc_fence_after();
-            const uint32_t d = tbase + kAccCol + b * 128;
-            if (j == 0) {
-              const uint32_t a = umma::smem_u32(base + InferTsSmem::feat + h * 16384);
-              umma::mma_bf16(d, umma::desc_sw128(a), umma::desc_sw128(w1d), idesc, 0);
-            } else {
-              const uint32_t bsm = umma::smem_u32(base + InferTsSmem::ring + slot * kChunkBytes);
-              // W4 chunks accumulate onto their bias, stored into TMEM by the epilogue.
-              const uint32_t acc0 = j >= 3 ? 1u : 0u;
-#pragma unroll
-              for (uint32_t k = 0; k < 8; ++k) {
-                const uint32_t off = (k >> 2) * 16384;
-                umma::mma_bf16_ts(d, tbase + h * 64 + k * 8, umma::desc_sw128(bsm + off) + 2 * (k & 3), idesc,
-                                  k | acc0);
-              }
-            }
-            umma::mma_commit(&acc_full[b]);
-          }
-          if (!ok) break;
-          if (j >= 1) {
-            umma::mma_commit(&ring_empty[slot]);
-            ++G;
-          }
-        }
-      }
-      umma::mma_commit(fin);
-    }
-  } else {
-    // Epilogue warps: half h of the 256-ray tile, TMEM lanes of quarter q.
-    const uint32_t e = warp - 2, h = e / 4, q = warp & 3;
-    const uint32_t row = q * 32 + lane;
-    uint8_t* feat = base + InferTsSmem::feat + h * 16384;
-    const uint32_t lane_base = (q * 32u) << 16;
-    const uint32_t a_col = tbase + lane_base + h * 64;  // this half's activations
-    uint32_t K = h;  // this half's jobs are K = h, h + 2, h + 4, ...
-    auto warp_wait = [&](uint64_t* bar, uint32_t parity) {
-      return __all_sync(0xffffffffu, umma::mbar_wait(bar, parity)) != 0;
-    };
-    if (!warp_wait(w_full, 0)) set_err(6);
-    for (uint32_t t = blockIdx.x; t < n_tiles && !failed(); t += gridDim.x) {
-      const uint32_t ray = t * 256 + h * 128 + row;
-      // Layer-1 operand: the 6 features (K = 16, rest zero) in panel 0.
-      {
-        float x[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (ray < p.n) ray_features(p.rays + size_t(ray) * 6, p.f, x);
-        __align__(16) bf16 v[16];
-#pragma unroll
-        for (int k = 0; k < 16; ++k) v[k] = __float2bfloat16_rn(k < 6 ? x[k] : 0.f);
-        *reinterpret_cast<uint4*>(feat + umma::sw128_offset(row, 0)) = *reinterpret_cast<const uint4*>(v);
-        *reinterpret_cast<uint4*>(feat + umma::sw128_offset(row, 8)) = *reinterpret_cast<const uint4*>(v + 8);
-      }
-      umma::fence_proxy_async();
-      __syncwarp();
-      if (lane == 0) umma::mbar_arrive(&act_ready[h]);
-      float best = -INFINITY;
-      uint32_t best_idx = 0;
-      for (uint32_t j = 0; j < jobs; ++j, K += 2) {
-        const uint32_t b = K % 3, u = K / 3;
-        if (!warp_wait(&acc_full[b], u & 1)) { set_err(7); break; }
-        umma::tc_fence_after();
-        const uint32_t tcol = tbase + lane_base + kAccCol + b * 128;
-        if (j < 3) {
-          // bias + ReLU -> bf16 pairs -> this half's activations in TMEM
-          const float* bb = s_bias + j * 128;
-          float v[128];
-          umma::tmem_ld128(tcol, v);
-          uint32_t o[64];
-#pragma unroll
-          for (int i = 0; i < 64; ++i) {
-            const __nv_bfloat162 pr = __floats2bfloat162_rn(fmaxf(v[2 * i] + bb[2 * i], 0.f),
-                                                            fmaxf(v[2 * i + 1] + bb[2 * i + 1], 0.f));
-            o[i] = *reinterpret_cast<const uint32_t*>(&pr);
-          }
-          umma::tmem_st64(a_col, o);
-        } else {
-          const uint32_t c0 = (j - 3) * 128;
-          float m = -INFINITY;
-          const bool full = c0 + 128 <= p.n_buckets;
-          const uint32_t r7f = *reinterpret_cast<volatile uint32_t*>(s_r7f);
-          float v[128];
-          umma::tmem_ld128(tcol, v);
-          if (full) {
-            float m1 = -INFINITY;
-#pragma unroll
-            for (uint32_t i = 0; i < 128; i += 4) {
-              const float k0 = tag7(v[i], r7f, i), k1 = tag7(v[i + 1], r7f, i + 1);
-              const float k2 = tag7(v[i + 2], r7f, i + 2), k3 = tag7(v[i + 3], r7f, i + 3);
-              m = umma::fmax3(m, k0, k1);
-              m1 = umma::fmax3(m1, k2, k3);
-            }
-            m = fmaxf(m, m1);
-          } else {
-#pragma unroll
-            for (uint32_t i = 0; i < 128; ++i) {
-              const float l = (c0 + i < p.n_buckets) ? v[i] : -INFINITY;
-              m = fmaxf(m, tag7(l, r7f, i));
-            }
-          }
-          if (m > best) {
-            best = m;
-            best_idx = c0 + (127u - (__float_as_uint(m) & 0x7Fu));
-          }
-        }
-        // Job K + 3 takes this accumulator next: if it is an output chunk,
-        // preload its bias (the same for every row, so this half's warps
-        // write it for whichever half that job belongs to).
-        const uint32_t jn = (j + (h == 0 ? 1u : 2u)) % jobs;
-        if (jn >= 3) {
-          const float* bb = s_bias + 384 + (jn - 3) * 128;
-          float v[128];
-#pragma unroll
-          for (int i = 0; i < 128; i += 4) {
-            const float4 q4 = *reinterpret_cast<const float4*>(bb + i);
-            v[i] = q4.x;
-            v[i + 1] = q4.y;
-            v[i + 2] = q4.z;
-            v[i + 3] = q4.w;
-          }
-          umma::tmem_st128(tcol, v);
-        }
-        umma::tc_fence_before();
-        __syncwarp();
-        if (lane == 0) {
-          umma::mbar_arrive(&acc_empty[b]);
-          if (j < 3) umma::mbar_arrive(&act_ready[h]);
-        }
-      }
-      if (ray < p.n && !failed()) p.out[ray] = int32_t(best_idx);
-    }
-  }
-  __syncwarp();
-  if (threadIdx.x == 32) {
-    if (!umma::mbar_wait(fin, 0)) set_err(8);
-  }
-  umma::tc_fence_before();
-  __syncthreads();
-  umma::tc_fence_after();
-  __syncwarp();
-  if (warp == 1) umma::tmem_dealloc(tbase, 512);
-  if (threadIdx.x == 0 && *s_err) atomicCAS(p.err, 0, *s_err);
-}
-
-// ---------------------------------------------------------------------------
 // TMA tensor maps (driver entry point fetched through the runtime).
 // ---------------------------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -1209,15 +941,10 @@ int32_t predict(sq_guide* g, const float* d_rays, uint32_t n, int32_t* d_bucket)
   static std::once_flag attr;
   std::call_once(attr, [] {
     cudaFuncSetAttribute(guide_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(InferSmem::bytes));
-    cudaFuncSetAttribute(guide_infer_ts_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(InferTsSmem::bytes));
   });
   const uint32_t tiles = (n + 255) / 256;
   const uint32_t grid = std::min<uint32_t>(tiles, uint32_t(ctx->sm_count));
-  static const bool ss = getenv("SQ_GUIDE_INFER_SS") != nullptr;  // A/B probe only
-  if (ss)
-    guide_infer_kernel<<<grid, kInferThreads, InferSmem::bytes, ctx->stream>>>(p);
-  else
-    guide_infer_ts_kernel<<<grid, kInferThreads, InferTsSmem::bytes, ctx->stream>>>(p);
+  guide_infer_kernel<<<grid, kInferThreads, InferSmem::bytes, ctx->stream>>>(p);
   ctx->launches++;
   CK(cudaGetLastError());
   return SQ_OK;

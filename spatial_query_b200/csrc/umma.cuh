@@ -133,19 +133,6 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint6
       : "memory");
 }
 
-// D[tmem] (+)= A[tmem] * B[smem]^T, one elected thread: the A operand is read
-// from tensor memory. For M = 128 and bf16, row m of A sits in TMEM lane m
-// and each 32-bit column holds two consecutive K elements (the lower K in
-// the low half), so one K = 16 step reads 8 columns starting at a_tmem.
-__device__ __forceinline__ void mma_bf16_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc,
-                                            uint32_t accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}" ::"r"(
-          d_tmem),
-      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-
 // Arrives once on `bar` when every tcgen05.mma this thread issued before has completed.
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
@@ -204,16 +191,6 @@ __device__ __forceinline__ void tmem_st128(uint32_t taddr, const float* v) {
       "tcgen05.st.sync.aligned.32x32b.x128.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63, %64, %65, %66, %67, %68, %69, %70, %71, %72, %73, %74, %75, %76, %77, %78, %79, %80, %81, %82, %83, %84, %85, %86, %87, %88, %89, %90, %91, %92, %93, %94, %95, %96, %97, %98, %99, %100, %101, %102, %103, %104, %105, %106, %107, %108, %109, %110, %111, %112, %113, %114, %115, %116, %117, %118, %119, %120, %121, %122, %123, %124, %125, %126, %127, %128};\n"
       "tcgen05.wait::st.sync.aligned;" ::"r"(taddr),
       "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]), "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]), "f"(v[16]), "f"(v[17]), "f"(v[18]), "f"(v[19]), "f"(v[20]), "f"(v[21]), "f"(v[22]), "f"(v[23]), "f"(v[24]), "f"(v[25]), "f"(v[26]), "f"(v[27]), "f"(v[28]), "f"(v[29]), "f"(v[30]), "f"(v[31]), "f"(v[32]), "f"(v[33]), "f"(v[34]), "f"(v[35]), "f"(v[36]), "f"(v[37]), "f"(v[38]), "f"(v[39]), "f"(v[40]), "f"(v[41]), "f"(v[42]), "f"(v[43]), "f"(v[44]), "f"(v[45]), "f"(v[46]), "f"(v[47]), "f"(v[48]), "f"(v[49]), "f"(v[50]), "f"(v[51]), "f"(v[52]), "f"(v[53]), "f"(v[54]), "f"(v[55]), "f"(v[56]), "f"(v[57]), "f"(v[58]), "f"(v[59]), "f"(v[60]), "f"(v[61]), "f"(v[62]), "f"(v[63]), "f"(v[64]), "f"(v[65]), "f"(v[66]), "f"(v[67]), "f"(v[68]), "f"(v[69]), "f"(v[70]), "f"(v[71]), "f"(v[72]), "f"(v[73]), "f"(v[74]), "f"(v[75]), "f"(v[76]), "f"(v[77]), "f"(v[78]), "f"(v[79]), "f"(v[80]), "f"(v[81]), "f"(v[82]), "f"(v[83]), "f"(v[84]), "f"(v[85]), "f"(v[86]), "f"(v[87]), "f"(v[88]), "f"(v[89]), "f"(v[90]), "f"(v[91]), "f"(v[92]), "f"(v[93]), "f"(v[94]), "f"(v[95]), "f"(v[96]), "f"(v[97]), "f"(v[98]), "f"(v[99]), "f"(v[100]), "f"(v[101]), "f"(v[102]), "f"(v[103]), "f"(v[104]), "f"(v[105]), "f"(v[106]), "f"(v[107]), "f"(v[108]), "f"(v[109]), "f"(v[110]), "f"(v[111]), "f"(v[112]), "f"(v[113]), "f"(v[114]), "f"(v[115]), "f"(v[116]), "f"(v[117]), "f"(v[118]), "f"(v[119]), "f"(v[120]), "f"(v[121]), "f"(v[122]), "f"(v[123]), "f"(v[124]), "f"(v[125]), "f"(v[126]), "f"(v[127])
-      : "memory");
-}
-
-// Stores 64 consecutive 32-bit columns of this thread's TMEM lane (32x32b
-// shape, same lane quarters as tmem_ld32) and waits for the store.
-__device__ __forceinline__ void tmem_st64(uint32_t taddr, const uint32_t* v) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x64.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63, %64};\n"
-      "tcgen05.wait::st.sync.aligned;" ::"r"(taddr),
-      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31]), "r"(v[32]), "r"(v[33]), "r"(v[34]), "r"(v[35]), "r"(v[36]), "r"(v[37]), "r"(v[38]), "r"(v[39]), "r"(v[40]), "r"(v[41]), "r"(v[42]), "r"(v[43]), "r"(v[44]), "r"(v[45]), "r"(v[46]), "r"(v[47]), "r"(v[48]), "r"(v[49]), "r"(v[50]), "r"(v[51]), "r"(v[52]), "r"(v[53]), "r"(v[54]), "r"(v[55]), "r"(v[56]), "r"(v[57]), "r"(v[58]), "r"(v[59]), "r"(v[60]), "r"(v[61]), "r"(v[62]), "r"(v[63])
       : "memory");
 }
 

@@ -177,13 +177,13 @@ def test_lists_casts_overlap_boxes(ctx, dim):
     casts = box_casts(rng, 4096, dim, -120.0, 120.0, 0.2, 3.0)
     lens = rng.range(0.0, 300.0, 4096).astype(np.float32)
     cn = o.shapecast_nearest(casts, lens)
-    assert (cn.leaf != O.NO_HIT).sum() > 50
+    assert (cn.leaf != O.NO_HIT).sum() > (50 if dim < 4 else 10)  # sparse in 6 dimensions
     same_nearest64(cn, g.shapecast_nearest(casts.astype(np.float64), lens.astype(np.float64)), f"cast D={dim}")
     same_lists64(o.shapecast_all(casts, lens, k=8), g.shapecast_all(casts.astype(np.float64), lens.astype(np.float64),
                                                                       k=8), f"cast all D={dim}")
     reg = regions(rng, 4096, dim, -100.0, 100.0, 0.5, 12.0)
     want = o.overlap(reg)
-    assert want[1].size > 100
+    assert want[1].size > (100 if dim < 4 else 10)
     got = g.overlap(reg.astype(np.float64))
     assert np.array_equal(want[0], got[0]) and np.array_equal(want[1], got[1]), f"overlap D={dim}"
     g.close()
