@@ -16,7 +16,8 @@
 // Inference (guide_infer_kernel): one persistent CTA per SM runs the whole
 // network for 256 rays at a time: warp 0 streams pre-swizzled weight chunks
 // (W2, W3, then W4 in 128-row chunks) with bulk copies into a 3-slot ring,
-// warp 1 issues tcgen05.mma into a double-buffered TMEM accumulator, eight
+// warps 1 and 10 issue tcgen05.mma (one thread each, one 128-ray half each)
+// into double-buffered TMEM accumulators, eight
 // epilogue warps apply bias + ReLU and write the next layer's bf16 operand
 // back to shared memory, and for the last layer fold each 128-logit chunk
 // into a running argmax. Logits never leave the SM.
@@ -273,7 +274,7 @@ __global__ void labels_kernel(const uint32_t* __restrict__ leaf, const int32_t* 
 // ---------------------------------------------------------------------------
 // Fused inference.
 // ---------------------------------------------------------------------------
-constexpr int kInferThreads = 320;  // warp 0 loads, warp 1 MMA, warps 2..9 epilogue
+constexpr int kInferThreads = 352;  // warp 0 loads, warps 1 and 10 issue MMAs (half 0 / half 1), warps 2..9 epilogue
 constexpr int kRing = 3;
 constexpr uint32_t kChunkBytes = 32768;  // 128 rows x 128 bf16, two swizzled panels
 
@@ -340,7 +341,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
     umma::mbar_init(w_full, 1);
     for (int s = 0; s < kRing; ++s) {
       umma::mbar_init(&ring_full[s], 1);
-      umma::mbar_init(&ring_empty[s], 1);
+      umma::mbar_init(&ring_empty[s], 2);  // released by both halves' MMAs
     }
     for (int k = 0; k < 4; ++k) {
       umma::mbar_init(&acc_full[k], 1);
@@ -348,7 +349,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
     }
     umma::mbar_init(&act_ready[0], 4);
     umma::mbar_init(&act_ready[1], 4);
-    umma::mbar_init(fin, 1);
+    umma::mbar_init(fin, 2);
     *s_err = 0;
     *s_r7f = 0x7Fu;
     umma::fence_barrier_init();
@@ -386,12 +387,17 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
         umma::mbar_wait(&ring_full[k % kRing], (k / kRing) & 1, 100000000ull);
       umma::mbar_wait(w_full, 0, 100000000ull);
     }
-  } else if (warp == 1) {
+  } else if (warp == 1 || warp == 10) {
     if (lane == 0) {
-      // MMA issuer.
+      // MMA issuers, one per half (warp 1: half 0, warp 10: half 1). With
+      // one issuing thread for both halves the tensor pipe drained while that
+      // thread waited on the next weight slot and accumulator; two threads
+      // keep one half's MMAs queued while the other half's issuer waits.
+      const uint32_t h = warp == 1 ? 0u : 1u;
       if (!umma::mbar_wait(w_full, 0)) set_err(2);
-      uint32_t G = 0, J = 0, A[2] = {0u, 0u};
+      uint32_t G = 0, J = 0, A = 0;
       const uint32_t w1d = umma::smem_u32(base + InferSmem::w1);
+      const uint32_t a = umma::smem_u32(base + InferSmem::act + h * 32768);
       bool ok = true;
       for (uint32_t t = blockIdx.x; ok && t < n_tiles && !failed(); t += gridDim.x) {
         for (uint32_t j = 0; ok && j < 3 + p.n_chunks && !failed(); ++j, ++J) {
@@ -399,38 +405,34 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
           uint32_t slot = 0;
           if (j >= 1) {
             slot = G % kRing;
-            if (!umma::mbar_wait(&ring_full[slot], (G / kRing) & 1)) { set_err(5); break; }
+            if (!umma::mbar_wait(&ring_full[slot], (G / kRing) & 1)) { set_err(5); ok = false; break; }
           }
-          for (uint32_t h = 0; h < 2; ++h) {
-            // Layers 1-3 and the first W4 chunk wait for this half's operand rows.
-            if (j <= 3) {
-              if (!umma::mbar_wait(&act_ready[h], A[h] & 1)) { set_err(3); ok = false; break; }
-              ++A[h];
-            }
-            if (J >= 2 && !umma::mbar_wait(&acc_empty[s * 2 + h], ((J / 2) + 1) & 1)) {
-              set_err(4);
-              ok = false;
-              break;
-            }
-            umma::tc_fence_after();
-            const uint32_t d = tbase + s * 256 + h * 128;
-            const uint32_t a = umma::smem_u32(base + InferSmem::act + h * 32768);
-            if (j == 0) {
-              umma::mma_bf16(d, umma::desc_sw128(a), umma::desc_sw128(w1d), idesc, 0);
-            } else {
-              const uint32_t bsm = umma::smem_u32(base + InferSmem::ring + slot * kChunkBytes);
-              // W4 chunks accumulate onto their bias, stored into TMEM by the epilogue.
-              const uint32_t acc0 = j >= 3 ? 1u : 0u;
+          // Layers 1-3 and the first W4 chunk wait for this half's operand rows.
+          if (j <= 3) {
+            if (!umma::mbar_wait(&act_ready[h], A & 1)) { set_err(3); ok = false; break; }
+            ++A;
+          }
+          if (J >= 2 && !umma::mbar_wait(&acc_empty[s * 2 + h], ((J / 2) + 1) & 1)) {
+            set_err(4);
+            ok = false;
+            break;
+          }
+          umma::tc_fence_after();
+          const uint32_t d = tbase + s * 256 + h * 128;
+          if (j == 0) {
+            umma::mma_bf16(d, umma::desc_sw128(a), umma::desc_sw128(w1d), idesc, 0);
+          } else {
+            const uint32_t bsm = umma::smem_u32(base + InferSmem::ring + slot * kChunkBytes);
+            // W4 chunks accumulate onto their bias, stored into TMEM by the epilogue.
+            const uint32_t acc0 = j >= 3 ? 1u : 0u;
 #pragma unroll
-              for (uint32_t k = 0; k < 8; ++k) {
-                const uint32_t off = (k >> 2) * 16384;
-                umma::mma_bf16(d, umma::desc_sw128(a + off) + 2 * (k & 3), umma::desc_sw128(bsm + off) + 2 * (k & 3),
-                               idesc, k | acc0);
-              }
+            for (uint32_t k = 0; k < 8; ++k) {
+              const uint32_t off = (k >> 2) * 16384;
+              umma::mma_bf16(d, umma::desc_sw128(a + off) + 2 * (k & 3), umma::desc_sw128(bsm + off) + 2 * (k & 3),
+                             idesc, k | acc0);
             }
-            umma::mma_commit(&acc_full[s * 2 + h]);
           }
-          if (!ok) break;
+          umma::mma_commit(&acc_full[s * 2 + h]);
           if (j >= 1) {
             umma::mma_commit(&ring_empty[slot]);
             ++G;

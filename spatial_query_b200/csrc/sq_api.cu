@@ -95,7 +95,7 @@ int32_t nearest_core(sq_ctx* ctx, const sq_bvh* b, bool cast, const float* d_q, 
     return near_first_launch(ctx, b, b->ks.ray_nearest_wide, ref_fn, p, 3 * b->wdepth + 1);
   if (!cast && !stats && ctx->layout == SQ_LAYOUT_QUANT && b->n_wide && b->d_qnodes && b->ks.ray_nearest_quant)
     return near_first_launch(ctx, b, b->ks.ray_nearest_quant, ref_fn, p, 3 * b->wdepth + 1);
-  return near_first_launch(ctx, b, near_fn, ref_fn, p, b->depth);
+  return near_first_launch(ctx, b, near_fn, kReplayInKernel ? nullptr : ref_fn, p, b->depth);
 }
 
 int32_t list_core(sq_ctx* ctx, const sq_bvh* b, int kind, const float* d_q, uint32_t n, float max_toi,
@@ -1233,7 +1233,8 @@ int32_t sqi::seeded_nearest(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, u
     // The bucket's ancestors' other children wait on the stack (one per level
     // above the bucket) while the bucket is searched: no deeper than a plain
     // descent to the same node, so the tree's depth bounds the stack.
-    if ((rc = near_first_launch(ctx, b, b->ks.ray_nearest_seeded[st ? 1 : 0], b->ks.ray_nearest[1][st ? 1 : 0], p,
+    if ((rc = near_first_launch(ctx, b, b->ks.ray_nearest_seeded[st ? 1 : 0],
+                                kReplayInKernel ? nullptr : b->ks.ray_nearest[1][st ? 1 : 0], p,
                                 b->depth + 1)))
       return rc;
   }
@@ -1345,6 +1346,15 @@ int32_t sqi::pipelined(sq_ctx* ctx, uint32_t n, const std::function<int32_t(uint
 
 int32_t sqi::near_first_launch(sq_ctx* ctx, const sq_bvh* b, const void* fn, const void* ref_fn, QueryParams& p,
                                uint32_t stack) {
+  p.window = ctx->window;
+  if (!ref_fn) {
+    // The kernel answers its uncertified queries again itself; only their
+    // number is kept.
+    CK(cudaMemsetAsync(ctx->d_replays, 0, sizeof(uint32_t), ctx->stream));
+    p.replay_count = ctx->d_replays;
+    p.replay_list = nullptr;
+    return launch_persistent(ctx, fn, p, stack, p.n);
+  }
   // The replay list holds at most every query of the batch; it grows here,
   // outside any stream capture once a batch of this size has run.
   const size_t need = size_t(std::max<uint32_t>(p.n, 1)) * sizeof(uint32_t);

@@ -450,6 +450,7 @@ template <int D, int K> struct Lane {
   uint32_t top_code; // postponed-leaf walks: the stack's top entry, held in registers
   float top_t;
   bool has_top;
+  bool ref;          // this walk answers the query again in the crate's own order (unseeded, exact limit)
   int sp;
   bool fast;
   uint32_t best_leaf;
@@ -509,6 +510,13 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   // not depend on the order of the visits); the counting and reference-order
   // walks keep the crate's sequence.
   constexpr bool SPEC = SQ_POSTPONE_LEAVES && DETECT && !STATS && !WIDE;
+  // An uncertified answer is answered again by the same lane, in the crate's
+  // order over the child-pair records, at its next refill (no second launch
+  // walking a handful of rays while the GPU idles). Four-wide walks list
+  // such queries for a reference-order launch over the child-pair records.
+  constexpr bool INREPLAY = DETECT && !WIDE && !SPEC;
+  bool pending = false;
+  uint32_t pending_q = 0;
   const float kInf = __int_as_float(0x7f800000);
 
   // Box test of one child (or the root) against the lane's query: the slab
@@ -556,11 +564,26 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
     const uint32_t q = L.q;
     if constexpr (DETECT && N != kNarrowAabb) {
       // Certify the answer: not before its own primitive's AABB entry.
-      if (L.best_leaf != kNoHit) {
+      if (L.best_leaf != kNoHit && !L.ref) {
         float rec[PL::vec * 4];
         load_vec<PL::vec>(p.prims + size_t(L.best_pos) * PL::vec, rec);
-        if (L.best_t < prim_entry<D, N, kCast>(rec, L.r, L.pmin, L.pmax, L.fast))
-          p.replay_list[atomicAdd(p.replay_count, 1u)] = q;
+        if (L.best_t < prim_entry<D, N, kCast>(rec, L.r, L.pmin, L.pmax, L.fast)) {
+          if constexpr (INREPLAY) {
+            // Answered again by this lane in the crate's order; this walk's
+            // counters still count, its answer is not written.
+            pending = true;
+            pending_q = q;
+            if (p.replay_count) atomicAdd(p.replay_count, 1u);
+            if (STATS) {
+              c_vis += L.v_nodes;
+              c_nar += L.v_nar;
+              c_hit += L.v_hit;
+            }
+            return;
+          } else {
+            p.replay_list[atomicAdd(p.replay_count, 1u)] = q;
+          }
+        }
       }
     }
     if constexpr (kNearest) {
@@ -601,8 +624,9 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   };
 
   // Loads query q and tests the root. False when the query is already done.
-  auto start = [&](uint32_t q) -> bool {
+  auto start = [&](uint32_t q, bool ref) -> bool {
     L.q = q;
+    L.ref = ref;
     const float* src = p.queries + size_t(q) * QW;
 #pragma unroll
     for (int i = 0; i < D; ++i) {
@@ -651,7 +675,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
     float te;
     const bool hit_root = test_box(lo, hi, te);
     L.code_t = te;
-    if constexpr (SEED) {
+    if constexpr (SEED) if (!L.ref) {
       const int32_t bk = p.seed_bucket[q];
       if (hit_root && bk >= 0 && uint32_t(bk) < p.n_buckets) {
         const uint2 e = __ldg(p.buckets + bk);
@@ -741,7 +765,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
               if (L.best_leaf == kNoHit || hit_before(t, id, L.best_t, L.best_leaf)) {
                 L.best_leaf = id;
                 L.best_t = t;
-                if constexpr (DETECT) {
+                if (DETECT && !L.ref) {
                   L.limit = near_limit(t, p.window);
                   L.best_pos = pos;
                 } else {
@@ -813,7 +837,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
 
   for (;;) {
     // Refill the lanes without a query.
-    const bool need = !live && !exhausted;
+    const bool need = !live && !exhausted && !pending;
     const uint32_t need_mask = __ballot_sync(FULL, need);
     uint32_t qs = kNoHit;
     if (need_mask) {
@@ -827,8 +851,14 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
         else exhausted = true;
       }
     }
+    bool replay = false;
+    if (INREPLAY && pending) {
+      qs = pending_q;
+      pending = false;
+      replay = true;
+    }
     if (qs != kNoHit) {
-      live = start(qs);
+      live = start(qs, replay);
       if (!live) finish();
     }
     const uint32_t live_mask = __ballot_sync(FULL, live);
@@ -1008,7 +1038,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
         if (pa && pb) {
           // Reference order: child_a waits, child_b goes first. Near-first:
           // the smaller entry goes first.
-          const bool a_first = (REF || !kNearest || (SEED && p.far_first)) ? false : (ta <= tb);
+          const bool a_first = (REF || !kNearest || L.ref || (SEED && p.far_first)) ? false : (ta <= tb);
           s_code[L.sp * kThreads + tid] = a_first ? cb : ca;
           s_t[L.sp * kThreads + tid] = a_first ? tb : ta;
           ++L.sp;

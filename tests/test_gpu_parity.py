@@ -268,3 +268,30 @@ def test_per_query_max_toi(order):
     mt = Rng(13).range(0.0, 60.0, 512)
     assert_same_nearest(o.nearest(rays, mt), g.raycast_nearest(rays, mt))
     assert_same_lists(o.all(rays, mt, k=8), g.raycast_all(rays, mt, k=8))
+
+
+def test_uncertified_answers_are_answered_again():
+    """Flat triangles in z = const planes: the triangle test's toi can land an
+    ulp before the slab entry of the triangle's flat AABB, an answer the
+    near-first walk cannot certify. Those rays are answered again in the
+    crate's order (by the same lane, in the same launch); every answer is the
+    oracle's, for plain and seeded-free host and device calls alike."""
+    from spatial_query_b200.scenes import normalize_rows
+    rng = Rng(77)
+    n, m = 20000, 65536
+    z = np.floor(rng.range(0.0, 40.0, n)).astype(np.float32)
+    v0 = np.stack([rng.range(-50.0, 50.0, n), rng.range(-50.0, 50.0, n), z], 1)
+    v1 = v0 + np.stack([rng.range(0.5, 5.0, n), rng.range(-2.0, 2.0, n), np.zeros(n, np.float32)], 1)
+    v2 = v0 + np.stack([rng.range(-2.0, 2.0, n), rng.range(0.5, 5.0, n), np.zeros(n, np.float32)], 1)
+    prims = np.ascontiguousarray(np.concatenate([v0, v1, v2], 1), dtype=np.float32)
+    o = np.stack([rng.range(-60.0, 60.0, m), rng.range(-60.0, 60.0, m), np.full(m, 80.0, np.float32)], 1)
+    d = normalize_rows(np.stack([rng.range(-0.3, 0.3, m), rng.range(-0.3, 0.3, m), -np.ones(m, np.float32)], 1))
+    rays = np.ascontiguousarray(np.concatenate([o, d], 1), dtype=np.float32)
+    oscene, g = pair("tris", 3, prims)
+    ref = oscene.nearest(rays, 500.0)
+    assert (ref.leaf != O.NO_HIT).mean() > 0.3
+    ctx().set_order(sq.ORDER_NEAR_FIRST)
+    got = g.raycast_nearest(rays, 500.0)
+    assert ctx().last_replay_count > 0
+    assert_same_nearest(ref, got, label="flat triangles, near-first with replays")
+    g.close()
