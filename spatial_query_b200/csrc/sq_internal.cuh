@@ -103,7 +103,7 @@ using namespace sq;
 // Near-first nearest launch `fn` followed by the reference-order replay
 // (`ref_fn`) of the queries it could not certify; with `ref_fn` null the
 // kernel answers those queries again itself (sq_api.cu).
-constexpr bool kReplayInKernel = !SQ_POSTPONE_LEAVES;
+constexpr bool kReplayInKernel = SQ_REPLAY_IN_KERNEL && !SQ_POSTPONE_LEAVES;
 int32_t near_first_launch(sq_ctx* ctx, const sq_bvh* b, const void* fn, const void* ref_fn, QueryParams& p,
                           uint32_t stack);
 

@@ -73,6 +73,11 @@ constexpr int kThreads = 128;
 #ifndef SQ_REG_TOP
 #define SQ_REG_TOP 0
 #endif
+// Uncertified near-first answers answered again by the same lane (1) or
+// listed for a reference-order launch (0).
+#ifndef SQ_REPLAY_IN_KERNEL
+#define SQ_REPLAY_IN_KERNEL 1
+#endif
 constexpr int kMaxStack = 96;  // deepest tree accepted (96 KB of stack per block)
 
 template <int D> struct NodeLayout {
@@ -514,7 +519,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   // order over the child-pair records, at its next refill (no second launch
   // walking a handful of rays while the GPU idles). Four-wide walks list
   // such queries for a reference-order launch over the child-pair records.
-  constexpr bool INREPLAY = DETECT && !WIDE && !SPEC;
+  constexpr bool INREPLAY = SQ_REPLAY_IN_KERNEL && DETECT && !WIDE && !SPEC;
   bool pending = false;
   uint32_t pending_q = 0;
   const float kInf = __int_as_float(0x7f800000);
