@@ -73,10 +73,15 @@ constexpr int kThreads = 128;
 #ifndef SQ_REG_TOP
 #define SQ_REG_TOP 0
 #endif
-// Uncertified near-first answers answered again by the same lane (1) or
-// listed for a reference-order launch (0).
+// Uncertified near-first answers answered again by the same lane at its
+// next refill (1), or listed for a reference-order launch (0, the default).
+// The lane replay removes the second launch (about 20 us per 1,048,576-ray
+// call, the serial walk of the one or two listed rays) but measured 0.918 ms
+// against 0.619 ms for the child-pair walk of the terrain's rays, with the
+// same single replay in both: the replay state in the refill loop costs the
+// whole walk far more than the launch it saves.
 #ifndef SQ_REPLAY_IN_KERNEL
-#define SQ_REPLAY_IN_KERNEL 1
+#define SQ_REPLAY_IN_KERNEL 0
 #endif
 constexpr int kMaxStack = 96;  // deepest tree accepted (96 KB of stack per block)
 
