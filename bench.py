@@ -65,6 +65,10 @@ def parse():
     ap.add_argument("--epochs", type=int, default=8, help="guide training epochs (batch 8192, AdamW lr 1e-3)")
     ap.add_argument("--rays", type=int, default=1 << 20,
                     help="rays per step (half coherent, half incoherent); the metric is quoted at 1,048,576")
+    ap.add_argument("--case", default=None,
+                    choices=["plain", "quant", "seed", "all", "cast", "ref", "refit", "build", "train", "infer", "f64"],
+                    help="profiling: set up the terrain (or, for f64, 200,000 boxes) and launch the one kernel of this "
+                         "case once (after its set-up launches), for single-kernel ncu captures; --rays rays")
     ap.add_argument("--side-configs", type=int, default=1,
                     help="terrain, one GPU: also run the 10,000-box, two-level and D = 6 workloads and fold their "
                          "results into the line (0: skip)")
@@ -553,6 +557,78 @@ def bench_mixture(args):
     return line
 
 
+def profile_case(args):
+    """One kernel of interest launched once, for an ncu capture of one launch.
+    query_kernel launch order: plain / quant / ref / all / cast: the case's
+    own launch first; seed: the labelling walk (2 launches: near-first and
+    its replay) then the seeded walk; the tree-build, refit, training and
+    inference cases launch their kernels after the scene upload."""
+    import torch
+    import spatial_query_b200 as sq
+    from spatial_query_b200 import scenes
+    dev = torch.device("cuda", 0)
+    case, n = args.case, args.rays
+    if case == "f64":
+        b = scenes.boxes_scene(seed=70, n_boxes=200000, n_rays=65536)
+        ctx = sq.Context(0)
+        g64 = sq.Geometry("boxes", 3, b["prims"])
+        s64 = sq.DeviceBvh64(ctx, sq.HostBvh.build_f64(3, g64.world_aabbs_f64()), g64)
+        s64.raycast_all(b["rays"].astype(np.float64), b["max_toi"], k=16)
+        ctx.synchronize()
+        print("case f64 ok")
+        return
+    s = scenes.terrain_scene(seed=1)
+    half = len(s["rays"]) // 2
+    rays = np.ascontiguousarray(np.concatenate([s["rays"][: n // 2], s["rays"][half: half + n - n // 2]]))
+    geom = sq.Geometry("tris", 3, s["prims"])
+    ctx = sq.Context(0)
+    scene = sq.DeviceBvh(ctx, sq.HostBvh.build(geom), geom)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    torch.cuda.set_stream(stream)
+    d_rays = torch.from_numpy(rays).to(dev)
+    leaf = torch.empty(n, dtype=torch.int32, device=dev)
+    toi = torch.empty(n, device=dev)
+    nrm = torch.empty((n, 3), device=dev)
+    if case in ("plain", "quant"):
+        if case == "quant":
+            ctx.set_layout(sq.LAYOUT_QUANT)
+        scene.raycast_nearest_d(d_rays, n, s["max_toi"], leaf, toi, nrm)
+    elif case == "ref":
+        ctx.set_order(sq.ORDER_REFERENCE)
+        scene.raycast_nearest_d(d_rays, n, s["max_toi"], leaf, toi, nrm)
+    elif case == "all":
+        cnt = torch.empty(n, dtype=torch.int32, device=dev)
+        al = torch.empty((n, 16), dtype=torch.int32, device=dev)
+        at = torch.empty((n, 16), device=dev)
+        scene.raycast_all_d(d_rays, n, s["max_toi"], 16, cnt, al, at)
+    elif case == "cast":
+        rng = scenes.Rng(9)
+        lo, hi = s["prims"].reshape(-1, 3).min(axis=0), s["prims"].reshape(-1, 3).max(axis=0)
+        o = rng.range(0.0, 1.0, (n, 3)) * (hi - lo) + lo
+        o[:, 2] = hi[2] + 5.0
+        d = scenes.normalize_rows(np.concatenate([rng.range(-0.3, 0.3, (n, 2)), -np.ones((n, 1))], axis=1))
+        h = rng.range(0.2, 2.0, (n, 3))
+        casts = torch.from_numpy(np.ascontiguousarray(np.concatenate([o, d, -h, h], axis=1), dtype=np.float32)).to(dev)
+        scene.shapecast_nearest_d(casts, n, 500.0, leaf, toi, nrm)
+    elif case == "refit":
+        scene.refit_d(torch.from_numpy(s["prims"]).to(dev))
+    elif case == "build":
+        sq.tree_build_d(ctx, 3, torch.from_numpy(geom.world_aabbs()).to(dev), geom.leaf_count)
+    else:  # seed, train, infer
+        guide = sq.Guide(scene, seed=0)
+        lab = torch.empty(n, dtype=torch.int32, device=dev)
+        guide.label_d(d_rays, n, s["max_toi"], lab)
+        if case == "train":
+            guide.train_step_d(d_rays[:8192], lab[:8192])
+        else:
+            bk = torch.empty(n, dtype=torch.int32, device=dev)
+            guide.predict_d(d_rays, n, bk)
+            if case == "seed":
+                guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], leaf, toi, nrm, d_bucket=bk)
+    ctx.synchronize()
+    print(f"case {case} ok")
+
+
 def side_configs(args):
     """The other benchmark configurations, each run as its own --workload
     line would run it, folded into the headline line: value, time, CPU
@@ -577,6 +653,10 @@ def main():
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.case:
+        if rank == 0:
+            profile_case(args)
         return
     if args.workload != "terrain":
         if rank == 0:
