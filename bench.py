@@ -561,8 +561,9 @@ def profile_case(args):
     """One kernel of interest launched once, for an ncu capture of one launch.
     query_kernel launch order: plain / quant / ref / all / cast: the case's
     own launch first; seed: the labelling walk (2 launches: near-first and
-    its replay) then the seeded walk; the tree-build, refit, training and
-    inference cases launch their kernels after the scene upload."""
+    its replay) then the walk seeded with those labels, i.e. each ray's true
+    bucket; the tree-build, refit, training and inference cases launch their
+    kernels after the scene upload."""
     import torch
     import spatial_query_b200 as sq
     from spatial_query_b200 import scenes
@@ -620,11 +621,11 @@ def profile_case(args):
         guide.label_d(d_rays, n, s["max_toi"], lab)
         if case == "train":
             guide.train_step_d(d_rays[:8192], lab[:8192])
-        else:
+        elif case == "infer":
             bk = torch.empty(n, dtype=torch.int32, device=dev)
             guide.predict_d(d_rays, n, bk)
-            if case == "seed":
-                guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], leaf, toi, nrm, d_bucket=bk)
+        else:  # the seeded walk given each ray's true bucket (-1, no seed, for a miss)
+            guide.raycast_nearest_guided_d(d_rays, n, s["max_toi"], leaf, toi, nrm, d_bucket=lab)
     ctx.synchronize()
     print(f"case {case} ok")
 
