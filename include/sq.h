@@ -137,7 +137,11 @@ typedef struct sq_bvh_info {
 
 /* ---- context ---------------------------------------------------------------
  * Replaces GpuRaycaster::headless / new's device acquisition
- * (gpu/mod.rs:252-324): returns SQ_ERR_NO_DEVICE when there is no GPU. */
+ * (gpu/mod.rs:252-324): returns SQ_ERR_NO_DEVICE when there is no GPU.
+ * A context owns a stream, a scratch arena and a memory pool; the stream-
+ * ordered scratch of the device tree build, the overlap sort and the f64
+ * host-buffer overlap comes from that pool, which keeps its memory for the
+ * next call until sq_ctx_destroy. */
 int32_t sq_version(void);
 int32_t sq_ctx_create(int32_t device, sq_ctx** out);
 int32_t sq_ctx_destroy(sq_ctx* ctx);

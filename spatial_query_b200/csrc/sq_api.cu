@@ -177,6 +177,7 @@ extern "C" int32_t sq_ctx_create(int32_t device, sq_ctx** out) {
     if (ctx->d_counters) cudaFree(ctx->d_counters);
     if (ctx->d_stats) cudaFree(ctx->d_stats);
     if (ctx->d_replays) cudaFree(ctx->d_replays);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
     return SQ_ERR_CUDA;
@@ -191,6 +192,15 @@ extern "C" int32_t sq_ctx_create(int32_t device, sq_ctx** out) {
   if ((e = cudaMalloc(&ctx->d_stats, 4 * sizeof(unsigned long long))) != cudaSuccess) return bail(e, "stats");
   if ((e = cudaMalloc(&ctx->d_replays, sizeof(uint32_t))) != cudaSuccess) return bail(e, "replays");
   if ((e = cudaMemset(ctx->d_replays, 0, sizeof(uint32_t))) != cudaSuccess) return bail(e, "replays");
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  if ((e = cudaMemPoolCreate(&ctx->pool, &props)) != cudaSuccess) return bail(e, "memory pool");
+  uint64_t keep = ~uint64_t(0);
+  if ((e = cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess)
+    return bail(e, "memory pool");
   *out = ctx;
   return SQ_OK;
 }
@@ -199,6 +209,7 @@ extern "C" int32_t sq_ctx_destroy(sq_ctx* ctx) {
   if (!ctx) return SQ_OK;
   cudaSetDevice(ctx->device);
   if (ctx->own) cudaStreamSynchronize(ctx->own);
+  if (ctx->stream && ctx->stream != ctx->own) cudaStreamSynchronize(ctx->stream);
   if (ctx->lane) sq_ctx_destroy(ctx->lane);
   sqi::release_err_slot(ctx);
   if (ctx->arena.p) cudaFree(ctx->arena.p);
@@ -208,6 +219,7 @@ extern "C" int32_t sq_ctx_destroy(sq_ctx* ctx) {
   if (ctx->d_stats) cudaFree(ctx->d_stats);
   if (ctx->s_in) cudaStreamDestroy(ctx->s_in);
   if (ctx->s_out) cudaStreamDestroy(ctx->s_out);
+  if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
   return SQ_OK;
@@ -1244,7 +1256,7 @@ int32_t sqi::seeded_nearest(sq_ctx* ctx, const sq_bvh* b, const float* d_rays, u
 
 // Each query's CSR segment of leaves in ascending order: one segmented sort
 // over all segments (the fill pass appends in walk order), with scratch
-// taken from the stream-ordered allocator.
+// from the context's memory pool.
 int32_t sqi::sort_csr_segments(sq_ctx* ctx, uint32_t* d_leaves, uint64_t total, const uint64_t* d_offsets, uint32_t n) {
   if (total < 2) return SQ_OK;
   if (total > uint64_t(INT32_MAX)) return fail(ctx, SQ_ERR_CAPACITY, "more than 2^31 overlap results");
@@ -1254,7 +1266,7 @@ int32_t sqi::sort_csr_segments(sq_ctx* ctx, uint32_t* d_leaves, uint64_t total, 
   CK(cub::DeviceSegmentedSort::SortKeys(nullptr, temp_bytes, keys, int(total), int(n), beg, beg + 1, ctx->stream));
   const size_t alt_bytes = (size_t(total) * 4 + 255) & ~size_t(255);
   char* tmp = nullptr;
-  CK(cudaMallocAsync(reinterpret_cast<void**>(&tmp), alt_bytes + temp_bytes, ctx->stream));
+  CK(scratch_alloc(ctx, reinterpret_cast<void**>(&tmp), alt_bytes + temp_bytes));
   keys = cub::DoubleBuffer<uint32_t>(d_leaves, reinterpret_cast<uint32_t*>(tmp));
   cudaError_t e = cub::DeviceSegmentedSort::SortKeys(tmp + alt_bytes, temp_bytes, keys, int(total), int(n), beg, beg + 1,
                                                      ctx->stream);

@@ -831,8 +831,7 @@ extern "C" int32_t sq_overlap_f64(sq_ctx* ctx, const sq_bvh* b, const double* re
   // takes the arena for its counts.
   char* dq = nullptr;
   const size_t qb = (size_t(n) * 2 * D * 8 + 255) & ~size_t(255);
-  CK(cudaMallocAsync(reinterpret_cast<void**>(&dq), qb + (size_t(n) + 1) * 8 + size_t(leaf_capacity) * 4 + 16,
-                     ctx->stream));
+  CK(sqi::scratch_alloc(ctx, reinterpret_cast<void**>(&dq), qb + (size_t(n) + 1) * 8 + size_t(leaf_capacity) * 4 + 16));
   uint64_t* d_off = reinterpret_cast<uint64_t*>(dq + qb);
   uint32_t* d_lv = reinterpret_cast<uint32_t*>(dq + qb + (size_t(n) + 1) * 8);
   cudaError_t e = n ? cudaMemcpyAsync(dq, regions, size_t(n) * 2 * D * 8, cudaMemcpyHostToDevice, ctx->stream)

@@ -54,6 +54,7 @@ struct sq_ctx {
   sq_ctx* lane = nullptr;  // second compute lane of the chunked host-buffer calls (own stream and scratch; made on first use)
   uint64_t launches = 0;
   std::unordered_map<uint64_t, int> occ;  // (kernel, dynamic smem) -> resident blocks per SM
+  cudaMemPool_t pool = nullptr;  // stream-ordered scratch that stays reserved between calls (scratch_alloc)
 };
 
 // An uploaded scene: device records plus the host topology (kept for the
@@ -195,6 +196,15 @@ inline uint32_t prim_vec(int dim, int narrow) {
 inline uint32_t node_vec(int dim) { return (4 * dim + 2 + 3) / 4; }
 inline uint32_t wide_vec(int dim) { return (8 * dim + 4 + 3) / 4; }
 inline uint32_t quant_vec(int dim) { return (dim + (dim + 3) / 4 + 2 * dim + 4 + 3) / 4; }
+
+// Stream-ordered scratch on the context's stream from the context's own
+// memory pool. The pool keeps what is freed for the next call (no release
+// threshold); the device's default pool hands freed memory back to the
+// driver at every synchronisation, and mapping it again cost 1-5 ms per
+// call (197 ms once) in a D = 6 overlap query whose kernels take 2 ms.
+inline cudaError_t scratch_alloc(sq_ctx* ctx, void** p, size_t bytes) {
+  return cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream);
+}
 
 inline int32_t arena_reserve(sq_ctx* ctx, size_t bytes) {
   if (ctx->arena.cap >= bytes) return SQ_OK;

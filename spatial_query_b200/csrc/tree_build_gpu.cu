@@ -381,7 +381,7 @@ extern "C" int32_t sq_tree_build_d(sq_ctx* ctx, int32_t dim, uint32_t n, const f
                o_pre = cv.take(N2 * 4), o_ctr = cv.take(16), o_lv = cv.take(size_t(2) * (n_levels + 1) * 4),
                o_sort = cv.take(sort_bytes);
   char* base = nullptr;
-  CK(cudaMallocAsync(reinterpret_cast<void**>(&base), cv.off, st));
+  CK(sqi::scratch_alloc(ctx, reinterpret_cast<void**>(&base), cv.off));
   uint32_t* keys = reinterpret_cast<uint32_t*>(base + o_keys);
   uint32_t* idx = reinterpret_cast<uint32_t*>(base + o_idx0);
   uint32_t* idx_alt = reinterpret_cast<uint32_t*>(base + o_idx1);

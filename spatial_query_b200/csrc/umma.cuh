@@ -157,21 +157,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Stores 32 consecutive f32 columns of this thread's TMEM lane (same lane
-// quarters as tmem_ld32) and waits for the store.
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float* v) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};\n"
-      "tcgen05.wait::st.sync.aligned;" ::"r"(taddr),
-      "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]), "f"(v[9]),
-      "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]), "f"(v[16]), "f"(v[17]), "f"(v[18]),
-      "f"(v[19]), "f"(v[20]), "f"(v[21]), "f"(v[22]), "f"(v[23]), "f"(v[24]), "f"(v[25]), "f"(v[26]), "f"(v[27]),
-      "f"(v[28]), "f"(v[29]), "f"(v[30]), "f"(v[31])
-      : "memory");
-}
-
-
 // 128 consecutive f32 columns of this thread's TMEM lane in one load, waited for.
 __device__ __forceinline__ void tmem_ld128(uint32_t taddr, float* v) {
   uint32_t r[128];
@@ -183,22 +168,6 @@ __device__ __forceinline__ void tmem_ld128(uint32_t taddr, float* v) {
       : "memory");
 #pragma unroll
   for (int i = 0; i < 128; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-// Stores 128 consecutive f32 columns of this thread's TMEM lane in one store and waits for it.
-__device__ __forceinline__ void tmem_st128(uint32_t taddr, const float* v) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x128.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63, %64, %65, %66, %67, %68, %69, %70, %71, %72, %73, %74, %75, %76, %77, %78, %79, %80, %81, %82, %83, %84, %85, %86, %87, %88, %89, %90, %91, %92, %93, %94, %95, %96, %97, %98, %99, %100, %101, %102, %103, %104, %105, %106, %107, %108, %109, %110, %111, %112, %113, %114, %115, %116, %117, %118, %119, %120, %121, %122, %123, %124, %125, %126, %127, %128};\n"
-      "tcgen05.wait::st.sync.aligned;" ::"r"(taddr),
-      "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]), "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]), "f"(v[16]), "f"(v[17]), "f"(v[18]), "f"(v[19]), "f"(v[20]), "f"(v[21]), "f"(v[22]), "f"(v[23]), "f"(v[24]), "f"(v[25]), "f"(v[26]), "f"(v[27]), "f"(v[28]), "f"(v[29]), "f"(v[30]), "f"(v[31]), "f"(v[32]), "f"(v[33]), "f"(v[34]), "f"(v[35]), "f"(v[36]), "f"(v[37]), "f"(v[38]), "f"(v[39]), "f"(v[40]), "f"(v[41]), "f"(v[42]), "f"(v[43]), "f"(v[44]), "f"(v[45]), "f"(v[46]), "f"(v[47]), "f"(v[48]), "f"(v[49]), "f"(v[50]), "f"(v[51]), "f"(v[52]), "f"(v[53]), "f"(v[54]), "f"(v[55]), "f"(v[56]), "f"(v[57]), "f"(v[58]), "f"(v[59]), "f"(v[60]), "f"(v[61]), "f"(v[62]), "f"(v[63]), "f"(v[64]), "f"(v[65]), "f"(v[66]), "f"(v[67]), "f"(v[68]), "f"(v[69]), "f"(v[70]), "f"(v[71]), "f"(v[72]), "f"(v[73]), "f"(v[74]), "f"(v[75]), "f"(v[76]), "f"(v[77]), "f"(v[78]), "f"(v[79]), "f"(v[80]), "f"(v[81]), "f"(v[82]), "f"(v[83]), "f"(v[84]), "f"(v[85]), "f"(v[86]), "f"(v[87]), "f"(v[88]), "f"(v[89]), "f"(v[90]), "f"(v[91]), "f"(v[92]), "f"(v[93]), "f"(v[94]), "f"(v[95]), "f"(v[96]), "f"(v[97]), "f"(v[98]), "f"(v[99]), "f"(v[100]), "f"(v[101]), "f"(v[102]), "f"(v[103]), "f"(v[104]), "f"(v[105]), "f"(v[106]), "f"(v[107]), "f"(v[108]), "f"(v[109]), "f"(v[110]), "f"(v[111]), "f"(v[112]), "f"(v[113]), "f"(v[114]), "f"(v[115]), "f"(v[116]), "f"(v[117]), "f"(v[118]), "f"(v[119]), "f"(v[120]), "f"(v[121]), "f"(v[122]), "f"(v[123]), "f"(v[124]), "f"(v[125]), "f"(v[126]), "f"(v[127])
-      : "memory");
-}
-
-// max of three (PTX max.f32 with three sources, sm_100).
-__device__ __forceinline__ float fmax3(float a, float b, float c) {
-  float r;
-  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-  return r;
 }
 
 // Byte offset of element (row, k) (k < 64) in a K-major 128-byte-swizzle
