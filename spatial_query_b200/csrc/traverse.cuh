@@ -83,6 +83,16 @@ constexpr int kThreads = 128;
 #ifndef SQ_REPLAY_IN_KERNEL
 #define SQ_REPLAY_IN_KERNEL 0
 #endif
+// Child order by warp vote (1) in the certified near-first walk: the lanes
+// that open the same record with both children hit take the order most of
+// them prefer (a __match_any_sync group and a ballot), so lanes that agree
+// on a node stay on the same path; 0 (the default): each lane's own nearer
+// child first. Measured on the terrain's 1,048,576 rays (answers identical):
+// 0.652 ms against 0.616 ms for each lane's own order; the vote costs every
+// node step, and a lane outvoted takes its farther child first.
+#ifndef SQ_WARP_ORDER
+#define SQ_WARP_ORDER 0
+#endif
 constexpr int kMaxStack = 96;  // deepest tree accepted (96 KB of stack per block)
 
 template <int D> struct NodeLayout {
@@ -1048,7 +1058,16 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
         if (pa && pb) {
           // Reference order: child_a waits, child_b goes first. Near-first:
           // the smaller entry goes first.
-          const bool a_first = (REF || !kNearest || L.ref || (SEED && p.far_first)) ? false : (ta <= tb);
+          bool a_first = (REF || !kNearest || L.ref || (SEED && p.far_first)) ? false : (ta <= tb);
+          if constexpr (SQ_WARP_ORDER && DETECT && !WIDE) {
+            const bool voter = !L.ref && !(SEED && p.far_first);
+            const uint32_t voters = __ballot_sync(__activemask(), voter);
+            if (voter) {
+              const uint32_t same = __match_any_sync(voters, L.code);
+              const uint32_t yes = __ballot_sync(voters, a_first) & same;
+              a_first = 2 * __popc(yes) >= __popc(same);
+            }
+          }
           s_code[L.sp * kThreads + tid] = a_first ? cb : ca;
           s_t[L.sp * kThreads + tid] = a_first ? tb : ta;
           ++L.sp;

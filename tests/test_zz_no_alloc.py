@@ -5,8 +5,9 @@ owns a fixed device-memory budget and forbids driver allocations, a
 real-time loop that cannot take an allocation's latency, code that holds no
 sq_ctx. sq_overlap_noalloc keeps its scratch in a static device array of the
 library instead. This test calls it through the C ABI twice in a row and
-checks both results against the ordinary overlap entry point bit for bit
-(overlap sets are integer results, so the tolerance is exact equality), and
+checks both results against the ordinary overlap entry point bit for bit,
+which in turn equals the oracle's CSR result (overlap sets are integer
+results, so the tolerance is exact equality), and
 checks that a batch beyond the array's capacity is refused. It creates its
 own context and scene, so it passes alone in a fresh process as well as
 after the other tests.
@@ -18,6 +19,7 @@ import pytest
 
 import spatial_query_b200 as sq
 from spatial_query_b200 import scenes
+from gpu_util import O
 
 pytestmark = pytest.mark.gpu
 
@@ -58,6 +60,9 @@ def test_overlap_noalloc_matches_overlap_twice():
     scene = sq.DeviceBvh(ctx, sq.HostBvh.build(geom), geom)
     want_off, want_leaves = scene.overlap(s["regions"])
     assert want_leaves.size > 0
+    # The oracle (the crate's CPU walk) gives the same CSR result.
+    o_off, o_leaves = O.Scene("boxes", 6, s["prims"]).overlap(s["regions"])
+    assert np.array_equal(o_off, want_off) and np.array_equal(o_leaves, want_leaves)
 
     dev = torch.device("cuda", 0)
     n = s["regions"].shape[0]
