@@ -418,6 +418,20 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
       uint32_t G = 0, J = 0, A = 0;
       const uint32_t w1d = umma::smem_u32(base + InferSmem::w1);
       const uint32_t a = umma::smem_u32(base + InferSmem::act + h * 32768);
+      // Every descriptor of the K-steps, made once: this half's operand rows
+      // and each weight slot. The epilogue warps keep the ALU pipe busy with
+      // the argmax; descriptor arithmetic between the MMAs would queue behind
+      // it and slow their issue.
+      static_assert(kRing == 3, "the issue below names each slot's descriptors");
+      uint64_t ad[8], bd[kRing][8];
+#pragma unroll
+      for (uint32_t k = 0; k < 8; ++k) {
+        const uint32_t off = (k >> 2) * 16384;
+        ad[k] = umma::desc_sw128(a + off) + 2 * (k & 3);
+#pragma unroll
+        for (int sl = 0; sl < kRing; ++sl)
+          bd[sl][k] = umma::desc_sw128(umma::smem_u32(base + InferSmem::ring + sl * kChunkBytes) + off) + 2 * (k & 3);
+      }
       bool ok = true;
       for (uint32_t t = blockIdx.x; ok && t < n_tiles && !failed(); t += gridDim.x) {
         for (uint32_t j = 0; ok && j < 3 + p.n_chunks && !failed(); ++j, ++J) {
@@ -441,14 +455,12 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
           const uint32_t d = tbase + s * 256 + h * 128;
           if (j == 0) {
             umma::mma_bf16(d, umma::desc_sw128(a), umma::desc_sw128(w1d), idesc, 0);
+          } else if (slot == 0) {
+            umma::mma_bf16_x8(d, ad, bd[0], idesc);
+          } else if (slot == 1) {
+            umma::mma_bf16_x8(d, ad, bd[1], idesc);
           } else {
-            const uint32_t bsm = umma::smem_u32(base + InferSmem::ring + slot * kChunkBytes);
-#pragma unroll
-            for (uint32_t k = 0; k < 8; ++k) {
-              const uint32_t off = (k >> 2) * 16384;
-              umma::mma_bf16(d, umma::desc_sw128(a + off) + 2 * (k & 3), umma::desc_sw128(bsm + off) + 2 * (k & 3),
-                             idesc, k);
-            }
+            umma::mma_bf16_x8(d, ad, bd[2], idesc);
           }
           umma::mma_commit(&acc_full[s * 2 + h]);
           if (j >= 1) {

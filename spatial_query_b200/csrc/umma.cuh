@@ -133,6 +133,25 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint6
       : "memory");
 }
 
+// Eight K-steps onto one accumulator: D = A0 B0^T (overwrite), then D +=
+// Ak Bk^T for k = 1..7, with every descriptor given (no arithmetic between
+// the instructions, so the issue does not wait on a busy ALU pipe).
+__device__ __forceinline__ void mma_bf16_x8(uint32_t d_tmem, const uint64_t* a, const uint64_t* b, uint32_t idesc) {
+  asm volatile(
+      "{\n .reg .pred p0, p1;\n setp.ne.b32 p0, %18, %18;\n setp.eq.b32 p1, %18, %18;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %2, %10, %1, p0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %3, %11, %1, p1;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %4, %12, %1, p1;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %5, %13, %1, p1;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %6, %14, %1, p1;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %7, %15, %1, p1;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %8, %16, %1, p1;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %9, %17, %1, p1;\n}" ::"r"(d_tmem),
+      "r"(idesc), "l"(a[0]), "l"(a[1]), "l"(a[2]), "l"(a[3]), "l"(a[4]), "l"(a[5]), "l"(a[6]), "l"(a[7]), "l"(b[0]),
+      "l"(b[1]), "l"(b[2]), "l"(b[3]), "l"(b[4]), "l"(b[5]), "l"(b[6]), "l"(b[7]), "r"(0u)
+      : "memory");
+}
+
 // Arrives once on `bar` when every tcgen05.mma this thread issued before has completed.
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
