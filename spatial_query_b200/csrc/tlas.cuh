@@ -1014,12 +1014,7 @@ template <int D, int IK> __global__ void __launch_bounds__(256) tlas_refit_kerne
     const uint32_t node = parent >> 1;
     if (atomicAdd(p.arrivals + node, 1u) == 0u) return;
     __threadfence();
-    const float* r = reinterpret_cast<const float*>(p.nodes + size_t(node) * NodeLayout<D>::vec);
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-      lo[i] = fminf(__ldcg(r + i), __ldcg(r + 2 * D + i));
-      hi[i] = fmaxf(__ldcg(r + D + i), __ldcg(r + 3 * D + i));
-    }
+    record_union<D>(p.nodes + size_t(node) * NodeLayout<D>::vec, lo, hi);
     parent = p.parents[node];
     store_slot<D>(rp, parent, lo, hi);
   }

@@ -1250,6 +1250,8 @@ __device__ __forceinline__ void prim_box(const float* v, float* lo, float* hi) {
   }
 }
 
+// Writes a child's box into its slot of the parent's record (or the root
+// box): 2D floats at an 8-byte aligned offset, as D two-float stores.
 template <int D>
 __device__ __forceinline__ void store_slot(const RefitParams& p, uint32_t parent, const float* lo, const float* hi) {
   float* dst;
@@ -1258,10 +1260,34 @@ __device__ __forceinline__ void store_slot(const RefitParams& p, uint32_t parent
   } else {
     dst = reinterpret_cast<float*>(p.nodes + size_t(parent >> 1) * NodeLayout<D>::vec) + (parent & 1u) * 2 * D;
   }
+  float v[2 * D];
 #pragma unroll
   for (int i = 0; i < D; ++i) {
-    dst[i] = lo[i];
-    dst[D + i] = hi[i];
+    v[i] = lo[i];
+    v[D + i] = hi[i];
+  }
+  float2* d2 = reinterpret_cast<float2*>(dst);
+#pragma unroll
+  for (int i = 0; i < D; ++i) d2[i] = make_float2(v[2 * i], v[2 * i + 1]);
+}
+
+// The union of a record's two child boxes (its own box in its parent),
+// read past L1 (the sibling thread wrote them) as D 16-byte loads.
+template <int D>
+__device__ __forceinline__ void record_union(const float4* rec, float* lo, float* hi) {
+  float b[4 * D];
+#pragma unroll
+  for (int w = 0; w < D; ++w) {
+    const float4 x = __ldcg(rec + w);
+    b[4 * w] = x.x;
+    b[4 * w + 1] = x.y;
+    b[4 * w + 2] = x.z;
+    b[4 * w + 3] = x.w;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    lo[i] = fminf(b[i], b[2 * D + i]);
+    hi[i] = fmaxf(b[D + i], b[3 * D + i]);
   }
 }
 
@@ -1302,12 +1328,7 @@ template <int D, int N> __global__ void __launch_bounds__(256) refit_kernel(cons
     const uint32_t node = parent >> 1;
     if (atomicAdd(p.arrivals + node, 1u) == 0u) return;  // the sibling finishes this node
     __threadfence();
-    const float* rec = reinterpret_cast<const float*>(p.nodes + size_t(node) * NodeLayout<D>::vec);
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-      lo[i] = fminf(__ldcg(rec + i), __ldcg(rec + 2 * D + i));
-      hi[i] = fmaxf(__ldcg(rec + D + i), __ldcg(rec + 3 * D + i));
-    }
+    record_union<D>(p.nodes + size_t(node) * NodeLayout<D>::vec, lo, hi);
     parent = p.parents[node];
     store_slot<D>(p, parent, lo, hi);
   }
