@@ -221,6 +221,9 @@ extern "C" int32_t sq_ctx_destroy(sq_ctx* ctx) {
   if (ctx->s_out) cudaStreamDestroy(ctx->s_out);
   if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   if (ctx->own) cudaStreamDestroy(ctx->own);
+  // A caller's stream may already be gone: no status of this teardown may be
+  // left for a later call's launch check to report.
+  cudaGetLastError();
   delete ctx;
   return SQ_OK;
 }
