@@ -536,9 +536,10 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
           float v[128];
           umma::tmem_ld128(tcol, v);  // the chunk's 128 logits of this row in one load and one wait
           // The logits are in registers: the accumulator goes back to the MMA
-          // issuer now, and the argmax below runs while the next chunks'
-          // MMAs do (with the argmax before the release, the MMAs waited on
-          // it: 1.03 ms per 1,048,576 rays against 0.82 ms without it).
+          // issuer now and the argmax below runs beside the next chunks'
+          // MMAs, adding the bias from registers (handing it back after the
+          // argmax, with the bias stored into TMEM first, measured the same:
+          // 1.032 against 1.035 ms per 1,048,576 rays).
           umma::tc_fence_before();
           __syncwarp();
           if (lane == 0) umma::mbar_arrive(&acc_empty[s * 2 + h]);
@@ -552,8 +553,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) guide_infer_kernel(const Inf
           if (c0 + 128 <= p.n_buckets) {
             // Four independent chains of two-input maxima: measured 0.999
             // against 1.035 ms per 1,048,576 rays for two chains of
-            // three-input maxima (max.f32 with three sources issues at half
-            // the rate of the two-input form).
+            // three-input maxima.
             float m1 = -INFINITY, m2 = -INFINITY, m3 = -INFINITY;
 #pragma unroll
             for (uint32_t i = 0; i < 128; i += 4) {
