@@ -80,6 +80,9 @@ extern "C" {
                                    the record's corner, rounded outward (64 B per record at D = 3, as a
                                    child-pair record); the exact records serve scenes with non-finite
                                    bounds */
+#define SQ_LAYOUT_BINARY_REGTOP 3 /* child-pair records walked with postponed leaves (a lane that reaches a
+                                   leaf keeps descending until its warp holds leaves) and the stack's top
+                                   entry in registers, older entries spilling to the shared-memory stack */
 
 typedef struct sq_ctx sq_ctx;
 typedef struct sq_bvh sq_bvh;
@@ -165,9 +168,10 @@ int32_t sq_ctx_set_replay_window(sq_ctx* ctx, float window);
  * configuration on a sample of device-resident rays (CUDA events, best of
  * `reps`), keeps the fastest in the context and reports the table. The knobs
  * are the traversal order (near-first, certified / the reference's order,
- * both give the reference's hits), the node records near-first walks
- * (child-pair, four-wide, quantised four-wide) and the persistent grid's
- * resident blocks per SM (0 = the occupancy limit): up to 32 entries. No counterpart in the reference, whose
+ * both give the reference's hits), the node records and walk of near-first
+ * rays (child-pair, four-wide, quantised four-wide, child-pair with the
+ * register-held stack top) and the persistent grid's resident blocks per SM
+ * (0 = the occupancy limit): up to 40 entries. No counterpart in the reference, whose
  * WGSL path has a fixed 64-thread workgroup (gpu/mod.rs:119-227). */
 typedef struct sq_tune_entry {
   int32_t order;
@@ -177,7 +181,7 @@ typedef struct sq_tune_entry {
 } sq_tune_entry;
 typedef struct sq_tune_result {
   uint32_t n_entries;
-  sq_tune_entry entries[32];
+  sq_tune_entry entries[40];
   int32_t best;  /* index into entries */
 } sq_tune_result;
 int32_t sq_autotune_nearest_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_rays, uint32_t n, float max_toi,

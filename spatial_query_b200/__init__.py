@@ -39,6 +39,7 @@ NO_HIT = 0xFFFFFFFF
 LAYOUT_BINARY = 0
 LAYOUT_WIDE = 1
 LAYOUT_QUANT = 2
+LAYOUT_BINARY_REGTOP = 3
 NO_SUB = 0xFFFFFFFF
 
 NARROW = {"boxes": 0, "aabb": 0, "balls": 1, "sphere": 1, "balls_near": 2, "sphere_near": 2, "tris": 3,
@@ -390,7 +391,8 @@ class Context:
         self.check(lib().sq_ctx_set_order(self.h, order), "set_order")
 
     def set_layout(self, layout: int):
-        """LAYOUT_BINARY (default), LAYOUT_WIDE or LAYOUT_QUANT node records for near-first rays."""
+        """LAYOUT_BINARY (default), LAYOUT_WIDE, LAYOUT_QUANT or LAYOUT_BINARY_REGTOP (child-pair records,
+        postponed leaves, the stack's top entry in registers) for near-first rays."""
         self.check(lib().sq_ctx_set_layout(self.h, layout), "set_layout")
 
     def set_replay_window(self, window: float):
@@ -490,7 +492,7 @@ class _TuneEntry(C.Structure):
 
 
 class _TuneResult(C.Structure):
-    _fields_ = [("n_entries", C.c_uint32), ("entries", _TuneEntry * 32), ("best", C.c_int32)]
+    _fields_ = [("n_entries", C.c_uint32), ("entries", _TuneEntry * 40), ("best", C.c_int32)]
 
 
 class DeviceBvh:

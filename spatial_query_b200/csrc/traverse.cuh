@@ -57,7 +57,8 @@ enum QKind : int { kRayNearest = 0, kRayAll = 1, kCastNearest = 2, kCastAll = 3,
 constexpr int kThreads = 128;
 
 // Two walk variants, measured on the 1,048,576-triangle terrain and off by
-// default (each slower there):
+// default (each slower there; both together are also built as the WALK = 1
+// instantiation, SQ_LAYOUT_BINARY_REGTOP, which the autotuner can pick):
 //  * SQ_POSTPONE_LEAVES: a lane that reaches a leaf holds it and keeps
 //    descending until the whole warp holds leaves (Aila and Laine's
 //    speculative traversal): 0.697 ms against 0.621 ms per 1,048,576 rays;
@@ -498,7 +499,10 @@ template <int D, int K> struct Lane {
 // WIDE (near-first nearest rays, no counters, no seed): the walk reads the
 // four-wide records; a step tests up to four children, goes to the nearest
 // and stacks the others farthest first.
-template <int D, int N, int K, bool REF, bool STATS, bool SEED = false, bool WIDE = false, bool QUANT = false>
+// WALK = 1 (near-first nearest rays over child-pair records, no counters):
+// postponed leaves with the stack's top entry held in registers.
+template <int D, int N, int K, bool REF, bool STATS, bool SEED = false, bool WIDE = false, bool QUANT = false,
+          int WALK = 0>
 __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   static_assert(!WIDE || (K == kRayNearest && !REF && !STATS && !SEED), "four-wide walks serve near-first rays only");
   static_assert(!QUANT || WIDE, "quantised records are a four-wide layout");
@@ -529,7 +533,8 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   // Postponed leaves for the certified near-first walks (their answers do
   // not depend on the order of the visits); the counting and reference-order
   // walks keep the crate's sequence.
-  constexpr bool SPEC = SQ_POSTPONE_LEAVES && DETECT && !STATS && !WIDE;
+  constexpr bool SPEC = (SQ_POSTPONE_LEAVES || WALK == 1) && DETECT && !STATS && !WIDE;
+  constexpr bool kRegTop = SQ_REG_TOP || WALK == 1;
   // An uncertified answer is answered again by the same lane, in the crate's
   // order over the child-pair records, at its next refill (no second launch
   // walking a handful of rays while the GPU idles). Four-wide walks list
@@ -562,7 +567,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
   // Pops the next waiting child whose entry still lies within the limit
   // (exactly the reference's slab verdict at pop time). False: stack empty.
   auto pop = [&]() -> bool {
-    if constexpr (SPEC && SQ_REG_TOP) {
+    if constexpr (SPEC && kRegTop) {
       if (L.has_top) {
         L.has_top = false;
         L.code = L.top_code;
@@ -916,7 +921,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
                 const bool a_first = (SEED && p.far_first) ? false : (ta <= tb);
                 const uint32_t far_code = a_first ? cb : ca;
                 const float far_t = a_first ? tb : ta;
-                if (SQ_REG_TOP) {
+                if constexpr (kRegTop) {
                   if (L.has_top) {  // the register entry spills below the new one
                     s_code[L.sp * kThreads + tid] = L.top_code;
                     s_t[L.sp * kThreads + tid] = L.top_t;
@@ -1372,6 +1377,7 @@ struct KernelSet {
   const void* ray_nearest[2][2];  // [ref][stats]
   const void* ray_nearest_wide;   // near-first over the four-wide records
   const void* ray_nearest_quant;  // near-first over the quantised four-wide records
+  const void* ray_nearest_regtop; // near-first, postponed leaves, stack top in registers (WALK = 1)
   const void* wide_sync;          // refreshes four-wide boxes from the binary records
   const void* quant_sync;         // quantises the four-wide records again
   const void* ray_all[2];         // [stats]
@@ -1392,6 +1398,7 @@ template <int D, int N> KernelSet make_kernel_set() {
   s.ray_nearest[1][1] = (const void*)query_kernel<D, N, kRayNearest, true, true>;
   s.ray_nearest_wide = (const void*)query_kernel<D, N, kRayNearest, false, false, false, true>;
   s.ray_nearest_quant = (const void*)query_kernel<D, N, kRayNearest, false, false, false, true, true>;
+  s.ray_nearest_regtop = (const void*)query_kernel<D, N, kRayNearest, false, false, false, false, false, 1>;
   s.wide_sync = (const void*)wide_sync_kernel<D>;
   s.quant_sync = (const void*)quant_sync_kernel<D>;
   s.ray_all[0] = (const void*)query_kernel<D, N, kRayAll, true, false>;

@@ -1,6 +1,8 @@
-"""Four-wide node records (SQ_LAYOUT_WIDE, near-first nearest rays) and
-their quantised copies (SQ_LAYOUT_QUANT: child boxes as 8-bit steps rounded
-outward) against the child-pair records and the oracle: the same
+"""Four-wide node records (SQ_LAYOUT_WIDE, near-first nearest rays), their
+quantised copies (SQ_LAYOUT_QUANT: child boxes as 8-bit steps rounded
+outward) and the child-pair walk with postponed leaves and the stack's top
+entry in registers (SQ_LAYOUT_BINARY_REGTOP) against the child-pair records
+and the oracle: the same
 leaf, toi, normal and sub-object bit for bit on boxes in 2, 3, 4 and 6
 dimensions, balls, triangles, with per-ray limits and a layer filter, on
 trees whose root is a leaf or has leaf children, and after a device refit
@@ -24,7 +26,7 @@ def ctx():
     c.close()
 
 
-@pytest.fixture(params=[sq.LAYOUT_WIDE, sq.LAYOUT_QUANT], ids=["wide", "quant"])
+@pytest.fixture(params=[sq.LAYOUT_WIDE, sq.LAYOUT_QUANT, sq.LAYOUT_BINARY_REGTOP], ids=["wide", "quant", "regtop"])
 def layout(request):
     return request.param
 
