@@ -969,6 +969,9 @@ def main():
                                     "register_stack_top_best_ms": round(min((e["ms"] for e in tune["table"]
                                                                              if e["order"] == 0 and e["layout"] == 3),
                                                                             default=float("nan")), 4),
+                                    "warp_vote_order_best_ms": round(min((e["ms"] for e in tune["table"]
+                                                                          if e["order"] == 0 and e["layout"] == 4),
+                                                                         default=float("nan")), 4),
                                     "reference_best_ms": round(min(e["ms"] for e in tune["table"] if e["order"] == 1), 4)},
                        "all_hits_k16": {"value": round(world * n / (all_ms / 1000) / 1e6, 3), "unit": "Mrays/s",
                                         "ms_per_step": round(all_ms, 4),

@@ -83,6 +83,8 @@ extern "C" {
 #define SQ_LAYOUT_BINARY_REGTOP 3 /* child-pair records walked with postponed leaves (a lane that reaches a
                                    leaf keeps descending until its warp holds leaves) and the stack's top
                                    entry in registers, older entries spilling to the shared-memory stack */
+#define SQ_LAYOUT_BINARY_VOTE 4 /* child-pair records, child order by warp vote: the lanes opening the same
+                                   record with both children hit take the order most of them prefer */
 
 typedef struct sq_ctx sq_ctx;
 typedef struct sq_bvh sq_bvh;
@@ -170,8 +172,9 @@ int32_t sq_ctx_set_replay_window(sq_ctx* ctx, float window);
  * are the traversal order (near-first, certified / the reference's order,
  * both give the reference's hits), the node records and walk of near-first
  * rays (child-pair, four-wide, quantised four-wide, child-pair with the
- * register-held stack top) and the persistent grid's resident blocks per SM
- * (0 = the occupancy limit): up to 40 entries. No counterpart in the reference, whose
+ * register-held stack top, child-pair with the warp-vote child order) and
+ * the persistent grid's resident blocks per SM (0 = the occupancy limit):
+ * up to 48 entries. No counterpart in the reference, whose
  * WGSL path has a fixed 64-thread workgroup (gpu/mod.rs:119-227). */
 typedef struct sq_tune_entry {
   int32_t order;
@@ -181,7 +184,7 @@ typedef struct sq_tune_entry {
 } sq_tune_entry;
 typedef struct sq_tune_result {
   uint32_t n_entries;
-  sq_tune_entry entries[40];
+  sq_tune_entry entries[48];
   int32_t best;  /* index into entries */
 } sq_tune_result;
 int32_t sq_autotune_nearest_d(sq_ctx* ctx, const sq_bvh* bvh, const float* d_rays, uint32_t n, float max_toi,

@@ -40,6 +40,7 @@ LAYOUT_BINARY = 0
 LAYOUT_WIDE = 1
 LAYOUT_QUANT = 2
 LAYOUT_BINARY_REGTOP = 3
+LAYOUT_BINARY_VOTE = 4
 NO_SUB = 0xFFFFFFFF
 
 NARROW = {"boxes": 0, "aabb": 0, "balls": 1, "sphere": 1, "balls_near": 2, "sphere_near": 2, "tris": 3,
@@ -391,8 +392,9 @@ class Context:
         self.check(lib().sq_ctx_set_order(self.h, order), "set_order")
 
     def set_layout(self, layout: int):
-        """LAYOUT_BINARY (default), LAYOUT_WIDE, LAYOUT_QUANT or LAYOUT_BINARY_REGTOP (child-pair records,
-        postponed leaves, the stack's top entry in registers) for near-first rays."""
+        """LAYOUT_BINARY (default), LAYOUT_WIDE, LAYOUT_QUANT, LAYOUT_BINARY_REGTOP (child-pair records,
+        postponed leaves, the stack's top entry in registers) or LAYOUT_BINARY_VOTE (child-pair records,
+        child order by warp vote) for near-first rays."""
         self.check(lib().sq_ctx_set_layout(self.h, layout), "set_layout")
 
     def set_replay_window(self, window: float):
@@ -492,7 +494,7 @@ class _TuneEntry(C.Structure):
 
 
 class _TuneResult(C.Structure):
-    _fields_ = [("n_entries", C.c_uint32), ("entries", _TuneEntry * 40), ("best", C.c_int32)]
+    _fields_ = [("n_entries", C.c_uint32), ("entries", _TuneEntry * 48), ("best", C.c_int32)]
 
 
 class DeviceBvh:

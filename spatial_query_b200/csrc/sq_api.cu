@@ -97,6 +97,8 @@ int32_t nearest_core(sq_ctx* ctx, const sq_bvh* b, bool cast, const float* d_q, 
     return near_first_launch(ctx, b, b->ks.ray_nearest_quant, ref_fn, p, 3 * b->wdepth + 1);
   if (!cast && !stats && ctx->layout == SQ_LAYOUT_BINARY_REGTOP && b->ks.ray_nearest_regtop)
     return near_first_launch(ctx, b, b->ks.ray_nearest_regtop, ref_fn, p, b->depth);
+  if (!cast && !stats && ctx->layout == SQ_LAYOUT_BINARY_VOTE && b->ks.ray_nearest_vote)
+    return near_first_launch(ctx, b, b->ks.ray_nearest_vote, ref_fn, p, b->depth);
   return near_first_launch(ctx, b, near_fn, kReplayInKernel ? nullptr : ref_fn, p, b->depth);
 }
 
@@ -253,8 +255,7 @@ extern "C" int32_t sq_ctx_set_order(sq_ctx* ctx, int32_t order) {
 }
 
 extern "C" int32_t sq_ctx_set_layout(sq_ctx* ctx, int32_t layout) {
-  if (!ctx || (layout != SQ_LAYOUT_BINARY && layout != SQ_LAYOUT_WIDE && layout != SQ_LAYOUT_QUANT &&
-               layout != SQ_LAYOUT_BINARY_REGTOP))
+  if (!ctx || layout < SQ_LAYOUT_BINARY || layout > SQ_LAYOUT_BINARY_VOTE)
     return SQ_ERR_INVALID;
   ctx->layout = layout;
   return SQ_OK;
@@ -1425,21 +1426,22 @@ extern "C" int32_t sq_autotune_nearest_d(sq_ctx* ctx, const sq_bvh* b, const flo
   const int saved_order = ctx->order, saved_bps = ctx->blocks_per_sm, saved_layout = ctx->layout;
   // (order, layout): near-first over child-pair records, over four-wide
   // records and over quantised four-wide records (when the scene has them),
-  // over child-pair records with the register-held stack top, the reference
-  // order.
-  const int orders[5] = {SQ_ORDER_NEAR_FIRST, SQ_ORDER_NEAR_FIRST, SQ_ORDER_NEAR_FIRST, SQ_ORDER_NEAR_FIRST,
-                         SQ_ORDER_REFERENCE};
-  const int layouts[5] = {SQ_LAYOUT_BINARY, SQ_LAYOUT_WIDE, SQ_LAYOUT_QUANT, SQ_LAYOUT_BINARY_REGTOP,
-                          SQ_LAYOUT_BINARY};
+  // over child-pair records with the register-held stack top or the
+  // warp-vote child order, the reference order.
+  const int orders[6] = {SQ_ORDER_NEAR_FIRST, SQ_ORDER_NEAR_FIRST, SQ_ORDER_NEAR_FIRST, SQ_ORDER_NEAR_FIRST,
+                         SQ_ORDER_NEAR_FIRST, SQ_ORDER_REFERENCE};
+  const int layouts[6] = {SQ_LAYOUT_BINARY,        SQ_LAYOUT_WIDE,        SQ_LAYOUT_QUANT,
+                          SQ_LAYOUT_BINARY_REGTOP, SQ_LAYOUT_BINARY_VOTE, SQ_LAYOUT_BINARY};
   const int bps[8] = {0, 2, 4, 6, 8, 10, 12, 16};
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   float best = 0.f;
-  for (int oi = 0; oi < 5 && rc == SQ_OK; ++oi) {
+  for (int oi = 0; oi < 6 && rc == SQ_OK; ++oi) {
     if (layouts[oi] == SQ_LAYOUT_WIDE && !(b->n_wide && b->ks.ray_nearest_wide)) continue;
     if (layouts[oi] == SQ_LAYOUT_QUANT && !(b->n_wide && b->d_qnodes && b->ks.ray_nearest_quant)) continue;
     if (layouts[oi] == SQ_LAYOUT_BINARY_REGTOP && !b->ks.ray_nearest_regtop) continue;
+    if (layouts[oi] == SQ_LAYOUT_BINARY_VOTE && !b->ks.ray_nearest_vote) continue;
     for (int bi = 0; bi < 8 && rc == SQ_OK; ++bi) {
       ctx->order = orders[oi];
       ctx->layout = layouts[oi];

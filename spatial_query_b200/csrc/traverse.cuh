@@ -88,7 +88,8 @@ constexpr int kThreads = 128;
 // that open the same record with both children hit take the order most of
 // them prefer (a __match_any_sync group and a ballot), so lanes that agree
 // on a node stay on the same path; 0 (the default): each lane's own nearer
-// child first. Measured on the terrain's 1,048,576 rays (answers identical):
+// child first (WALK = 2 builds it as SQ_LAYOUT_BINARY_VOTE). Measured on the
+// terrain's 1,048,576 rays (answers identical):
 // 0.652 ms against 0.616 ms for each lane's own order; the vote costs every
 // node step, and a lane outvoted takes its farther child first.
 #ifndef SQ_WARP_ORDER
@@ -499,8 +500,9 @@ template <int D, int K> struct Lane {
 // WIDE (near-first nearest rays, no counters, no seed): the walk reads the
 // four-wide records; a step tests up to four children, goes to the nearest
 // and stacks the others farthest first.
-// WALK = 1 (near-first nearest rays over child-pair records, no counters):
-// postponed leaves with the stack's top entry held in registers.
+// WALK (near-first nearest rays over child-pair records, no counters): 1 =
+// postponed leaves with the stack's top entry held in registers; 2 = child
+// order by warp vote.
 template <int D, int N, int K, bool REF, bool STATS, bool SEED = false, bool WIDE = false, bool QUANT = false,
           int WALK = 0>
 __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
@@ -1064,7 +1066,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
           // Reference order: child_a waits, child_b goes first. Near-first:
           // the smaller entry goes first.
           bool a_first = (REF || !kNearest || L.ref || (SEED && p.far_first)) ? false : (ta <= tb);
-          if constexpr (SQ_WARP_ORDER && DETECT && !WIDE) {
+          if constexpr ((SQ_WARP_ORDER || WALK == 2) && DETECT && !WIDE) {
             const bool voter = !L.ref && !(SEED && p.far_first);
             const uint32_t voters = __ballot_sync(__activemask(), voter);
             if (voter) {
@@ -1378,6 +1380,7 @@ struct KernelSet {
   const void* ray_nearest_wide;   // near-first over the four-wide records
   const void* ray_nearest_quant;  // near-first over the quantised four-wide records
   const void* ray_nearest_regtop; // near-first, postponed leaves, stack top in registers (WALK = 1)
+  const void* ray_nearest_vote;   // near-first, child order by warp vote (WALK = 2)
   const void* wide_sync;          // refreshes four-wide boxes from the binary records
   const void* quant_sync;         // quantises the four-wide records again
   const void* ray_all[2];         // [stats]
@@ -1399,6 +1402,7 @@ template <int D, int N> KernelSet make_kernel_set() {
   s.ray_nearest_wide = (const void*)query_kernel<D, N, kRayNearest, false, false, false, true>;
   s.ray_nearest_quant = (const void*)query_kernel<D, N, kRayNearest, false, false, false, true, true>;
   s.ray_nearest_regtop = (const void*)query_kernel<D, N, kRayNearest, false, false, false, false, false, 1>;
+  s.ray_nearest_vote = (const void*)query_kernel<D, N, kRayNearest, false, false, false, false, false, 2>;
   s.wide_sync = (const void*)wide_sync_kernel<D>;
   s.quant_sync = (const void*)quant_sync_kernel<D>;
   s.ray_all[0] = (const void*)query_kernel<D, N, kRayAll, true, false>;

@@ -23,8 +23,8 @@ def test_autotune_keeps_hits_exact():
     torch.cuda.synchronize()
     res = scene.autotune_nearest_d(d_rays, n, s["max_toi"], reps=2)
     # near-first over child-pair, four-wide and quantised four-wide records, the reference order: 8 grids each
-    assert len(res["table"]) == 40
-    assert {(e["order"], e["layout"]) for e in res["table"]} == {(0, 0), (0, 1), (0, 2), (0, 3), (1, 0)}
+    assert len(res["table"]) == 48
+    assert {(e["order"], e["layout"]) for e in res["table"]} == {(0, 0), (0, 1), (0, 2), (0, 3), (0, 4), (1, 0)}
     assert all(e["ms"] > 0 for e in res["table"])
     assert res["best"]["ms"] == min(e["ms"] for e in res["table"])
     ref = O.Scene("tris", 3, s["prims"]).nearest(s["rays"], s["max_toi"])

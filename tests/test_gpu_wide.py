@@ -1,8 +1,9 @@
 """Four-wide node records (SQ_LAYOUT_WIDE, near-first nearest rays), their
 quantised copies (SQ_LAYOUT_QUANT: child boxes as 8-bit steps rounded
 outward) and the child-pair walk with postponed leaves and the stack's top
-entry in registers (SQ_LAYOUT_BINARY_REGTOP) against the child-pair records
-and the oracle: the same
+entry in registers (SQ_LAYOUT_BINARY_REGTOP) and the child-pair walk with
+the warp-vote child order (SQ_LAYOUT_BINARY_VOTE) against the child-pair
+records and the oracle: the same
 leaf, toi, normal and sub-object bit for bit on boxes in 2, 3, 4 and 6
 dimensions, balls, triangles, with per-ray limits and a layer filter, on
 trees whose root is a leaf or has leaf children, and after a device refit
@@ -26,7 +27,8 @@ def ctx():
     c.close()
 
 
-@pytest.fixture(params=[sq.LAYOUT_WIDE, sq.LAYOUT_QUANT, sq.LAYOUT_BINARY_REGTOP], ids=["wide", "quant", "regtop"])
+@pytest.fixture(params=[sq.LAYOUT_WIDE, sq.LAYOUT_QUANT, sq.LAYOUT_BINARY_REGTOP, sq.LAYOUT_BINARY_VOTE],
+                ids=["wide", "quant", "regtop", "vote"])
 def layout(request):
     return request.param
 
