@@ -166,6 +166,15 @@ int32_t sq_ctx_set_blocks_per_sm(sq_ctx* ctx, int32_t blocks);
  * slab entry of its own primitive's AABB (the one case where the reference's
  * walk could miss it). */
 int32_t sq_ctx_set_replay_window(sq_ctx* ctx, float window);
+/* Keeps a scene's node records in L2 across calls: marks them as persisting
+ * for kernels on the context's stream (and its internal second lane) through
+ * an access-policy window (persisting on a hit, streaming on a miss), with
+ * up to `bytes` of the L2 set aside for persisting lines (capped at the
+ * device's maximum; hit ratio = set-aside bytes / window bytes). The
+ * set-aside belongs to this process's CUDA context and ends with it. `bvh`
+ * NULL or `bytes` 0 clears the window and returns persisting lines to
+ * normal. Answers are unchanged; only where the records live changes. */
+int32_t sq_ctx_set_l2_persist(sq_ctx* ctx, const sq_bvh* bvh, uint64_t bytes);
 /* Autotuner for nearest rays on one scene: times every candidate launch
  * configuration on a sample of device-resident rays (CUDA events, best of
  * `reps`), keeps the fastest in the context and reports the table. The knobs

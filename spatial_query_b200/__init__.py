@@ -108,6 +108,7 @@ SIGNATURES = {
     "sq_ctx_launch_count": (C.c_uint64, [P]),
     "sq_ctx_last_replay_count": (C.c_int32, [P, C.POINTER(C.c_uint32)]),
     "sq_ctx_set_replay_window": (C.c_int32, [P, C.c_float]),
+    "sq_ctx_set_l2_persist": (C.c_int32, [P, P, C.c_uint64]),
     "sq_tree_build": (C.c_int32, [C.c_int32, C.c_uint32, P, C.c_int32, C.c_uint32, P, P, P, P, P, P]),
     "sq_prim_aabbs": (C.c_int32, [C.c_int32, C.c_int32, C.c_uint32, P, P]),
     "sq_tree_build_d": (C.c_int32, [P, C.c_int32, C.c_uint32, P, C.c_uint32, P, P, P, P, P, P]),
@@ -396,6 +397,11 @@ class Context:
         postponed leaves, the stack's top entry in registers) or LAYOUT_BINARY_VOTE (child-pair records,
         child order by warp vote) for near-first rays."""
         self.check(lib().sq_ctx_set_layout(self.h, layout), "set_layout")
+
+    def set_l2_persist(self, scene=None, nbytes: int = 0):
+        """Keep `scene`'s node records persisting in L2 (up to nbytes set aside); no scene or 0 clears it."""
+        self.check(lib().sq_ctx_set_l2_persist(self.h, scene.h if scene is not None else None, int(nbytes)),
+                   "set_l2_persist")
 
     def set_replay_window(self, window: float):
         self.check(lib().sq_ctx_set_replay_window(self.h, window), "set_replay_window")

@@ -236,9 +236,15 @@ extern "C" const char* sq_ctx_last_error(const sq_ctx* ctx) { return ctx ? ctx->
 
 extern "C" void* sq_ctx_stream(sq_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
+namespace {
+int32_t apply_l2_window(sq_ctx* ctx);
+}
+
 extern "C" int32_t sq_ctx_set_stream(sq_ctx* ctx, void* stream) {
   if (!ctx) return SQ_ERR_INVALID;
   ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+  // An L2 window set with sq_ctx_set_l2_persist follows the context's stream.
+  if (ctx->l2_window.num_bytes) return apply_l2_window(ctx);
   return SQ_OK;
 }
 
@@ -272,6 +278,45 @@ extern "C" uint64_t sq_ctx_launch_count(const sq_ctx* ctx) { return ctx ? ctx->l
 extern "C" int32_t sq_ctx_set_replay_window(sq_ctx* ctx, float window) {
   if (!ctx || !(window >= 0.f) || window > 1.f) return SQ_ERR_INVALID;
   ctx->window = window;
+  return SQ_OK;
+}
+
+namespace {
+int32_t apply_l2_window(sq_ctx* ctx) {
+  cudaStreamAttrValue v{};
+  v.accessPolicyWindow = ctx->l2_window;
+  CK(cudaStreamSetAttribute(ctx->stream, cudaStreamAttributeAccessPolicyWindow, &v));
+  return SQ_OK;
+}
+}  // namespace
+
+extern "C" int32_t sq_ctx_set_l2_persist(sq_ctx* ctx, const sq_bvh* b, uint64_t bytes) {
+  if (!ctx) return SQ_ERR_INVALID;
+  if (b && b->device != ctx->device) return fail(ctx, SQ_ERR_INVALID, "scene on another device");
+  CK(cudaSetDevice(ctx->device));
+  ctx->l2_window = cudaAccessPolicyWindow{};
+  if (b && bytes && b->d_nodes && b->n_interior) {
+    int max_persist = 0, max_window = 0;
+    CK(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, ctx->device));
+    CK(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, ctx->device));
+    if (max_persist <= 0 || max_window <= 0) return fail(ctx, SQ_ERR_UNSUPPORTED, "no persisting L2 on this device");
+    const size_t reserve = std::min<size_t>(bytes, size_t(max_persist));
+    CK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, reserve));
+    const size_t region = size_t(b->n_interior) * node_vec(b->dim) * 16;
+    const size_t win = std::min<size_t>(region, size_t(max_window));
+    ctx->l2_window.base_ptr = b->d_nodes;
+    ctx->l2_window.num_bytes = win;
+    ctx->l2_window.hitRatio = std::min(1.0f, float(double(reserve) / double(win)));
+    ctx->l2_window.hitProp = cudaAccessPropertyPersisting;
+    ctx->l2_window.missProp = cudaAccessPropertyStreaming;
+  }
+  int32_t rc = apply_l2_window(ctx);
+  if (rc == SQ_OK && ctx->lane) rc = apply_l2_window(ctx->lane);
+  if (rc) return rc;
+  if (ctx->l2_window.num_bytes == 0) {
+    // Lines marked persisting so far go back to normal.
+    CK(cudaCtxResetPersistingL2Cache());
+  }
   return SQ_OK;
 }
 
@@ -1297,6 +1342,11 @@ int32_t sqi::second_lane(sq_ctx* ctx, sq_ctx** out) {
   lane->blocks_per_sm = ctx->blocks_per_sm;
   lane->window = ctx->window;
   lane->layout = ctx->layout;
+  if (lane->l2_window.num_bytes != ctx->l2_window.num_bytes || lane->l2_window.base_ptr != ctx->l2_window.base_ptr) {
+    lane->l2_window = ctx->l2_window;
+    int32_t rc = apply_l2_window(lane);
+    if (rc) return fail(ctx, rc, lane->err.c_str());
+  }
   *out = lane;
   return SQ_OK;
 }

@@ -55,6 +55,7 @@ struct sq_ctx {
   uint64_t launches = 0;
   std::unordered_map<uint64_t, int> occ;  // (kernel, dynamic smem) -> resident blocks per SM
   cudaMemPool_t pool = nullptr;  // stream-ordered scratch that stays reserved between calls (scratch_alloc)
+  cudaAccessPolicyWindow l2_window{};  // sq_ctx_set_l2_persist (num_bytes 0: none)
 };
 
 // An uploaded scene: device records plus the host topology (kept for the
