@@ -785,14 +785,15 @@ size_t overlap_scratch_bytes(uint32_t n) {
   return al((size_t(n) + 1) * 4) + al(size_t(n) * 4 + 4) + al(size_t(n) + 1) + al(16) + overlap_scan_temp(n) + 256;
 }
 
-// Records a region may visit before the warp-per-region kernel takes it.
+// Records a region may visit before the block-per-region kernel takes it.
 constexpr uint32_t kOverlapVisitBudget = 256;
 
-// Launches overlap_heavy_kernel over the regions the count pass listed.
+// Launches overlap_heavy_kernel over the regions the count pass listed (a
+// block per region, one shared stack of 256 x (depth + 1) entries).
 int32_t launch_heavy(sq_ctx* ctx, const sq_bvh* b, QueryParams& p) {
-  const uint32_t cap = 64u * (b->depth + 1);
+  const uint32_t cap = 256u * (b->depth + 1);
   p.stack = int(cap);
-  const size_t smem = size_t(kHeavyWarps) * cap * 4;
+  const size_t smem = size_t(cap) * 4;
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(b->ks.overlap_heavy, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   void* args[] = {&p};
   CK(cudaLaunchKernel(b->ks.overlap_heavy, dim3(ctx->sm_count * 4), dim3(32 * kHeavyWarps), args, smem, ctx->stream));

@@ -270,7 +270,7 @@ struct QueryParams {
   int fill;  // overlap: 0 count, 1 fill in ascending order, 2 fill in walk order
   int far_first;  // seeded walks: after the bucket, the crate's child order (push a, push b) instead of near-first
   // Overlap regions that visit more than visit_budget records in the count
-  // pass are left to overlap_heavy_kernel (a warp per region): listed in
+  // pass are left to overlap_heavy_kernel (a block per region): listed in
   // heavy_list, flagged in heavy_flag (the fill pass skips them).
   uint32_t* heavy_list;
   uint32_t* heavy_count;
@@ -685,7 +685,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
     L.csr_base = 0;
     if constexpr (K == kOverlap) {
       if (p.fill) L.csr_base = p.csr_offsets[q];
-      if (p.fill && p.heavy_flag && p.heavy_flag[q]) return false;  // filled by the warp-per-region kernel
+      if (p.fill && p.heavy_flag && p.heavy_flag[q]) return false;  // filled by the block-per-region kernel
     }
     L.v_nodes = STATS ? 1u : 0u;
     L.v_nar = 0;
@@ -1053,7 +1053,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
         const bool pb = test_box(rec + 2 * D, rec + 3 * D, tb);
         if (STATS) L.v_nodes += 2;
         if constexpr (K == kOverlap) {
-          // A region heavier than the budget goes to the warp-per-region
+          // A region heavier than the budget goes to the block-per-region
           // kernel instead of holding the launch's tail on one thread.
           if (p.heavy_list && !p.fill && ++L.v_nar > p.visit_budget) {
             p.heavy_flag[L.q] = 1;
@@ -1115,18 +1115,20 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
 }
 
 // ---------------------------------------------------------------------------
-// Heavy overlap regions: one warp per region. The warp keeps the region's
-// pending nodes in a shared-memory stack and each step takes up to 32 of them
-// from the top, one per lane: an interior record's overlapping children are
-// pushed (warp prefix sum for the slots), a leaf's accepted overlapping
-// primitives are counted (count pass) or written to the region's CSR segment
-// in any order (fill pass; the segmented sort that follows orders them).
-// Any order of visits finds the same set of leaves as the crate's walk.
-// Stack: each step replaces the <= 32 entries it takes with <= 64 children one
-// level deeper, so at most 32 entries per level stay below the top: the
-// stack never holds more than 32 x (depth + 1) + 32 entries; it is sized
-// 64 x (depth + 1) per warp (dynamic shared memory), and a push past it is
-// refused and reported through heavy_count's high bit instead of written.
+// Heavy overlap regions: one block (128 threads) per region. The block keeps
+// the region's pending nodes in one shared-memory stack and each step takes
+// up to 128 of them from the top, one per thread: an interior record's
+// overlapping children are pushed (block prefix sum for the slots), a leaf's
+// accepted overlapping primitives are counted (count pass) or written to the
+// region's CSR segment in any order (fill pass; the segmented sort that
+// follows orders them). Any order of visits finds the same set of leaves as
+// the crate's walk. (A warp per region left the heaviest region's walk on 32
+// lanes: 339 us for the D = 6 mixture's count pass with 5% of warp slots
+// busy.) Stack: each step replaces the <= 128 entries it takes with <= 256
+// children one level deeper, so at most 128 entries per level stay below the
+// top: it never holds more than 128 x (depth + 2) entries; it is sized
+// 256 x (depth + 1) (dynamic shared memory), and a push past it is refused
+// and reported through heavy_count's high bit instead of written.
 // ---------------------------------------------------------------------------
 constexpr int kHeavyWarps = 4;
 
@@ -1135,13 +1137,16 @@ __global__ void __launch_bounds__(32 * kHeavyWarps) overlap_heavy_kernel(const Q
   using PL = PrimLayout<D, N>;
   using NL = NodeLayout<D>;
   constexpr uint32_t FULL = 0xffffffffu;
-  extern __shared__ uint32_t heavy_smem[];
-  __shared__ unsigned long long s_fill[kHeavyWarps];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int cap = p.stack;  // entries per warp
-  uint32_t* stk = heavy_smem + size_t(w) * cap;
+  constexpr int T = 32 * kHeavyWarps;
+  extern __shared__ uint32_t stk[];
+  __shared__ unsigned long long s_fill;
+  __shared__ int s_sp;
+  __shared__ int s_wsum[kHeavyWarps];
+  __shared__ uint32_t s_count[kHeavyWarps];
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const int cap = p.stack;  // entries
   const uint32_t nh = *p.heavy_count & 0x7FFFFFFFu;
-  for (uint32_t i = blockIdx.x * kHeavyWarps + w; i < nh; i += gridDim.x * kHeavyWarps) {
+  for (uint32_t i = blockIdx.x; i < nh; i += gridDim.x) {
     const uint32_t q = p.heavy_list[i];
     float lo[D], hi[D];
 #pragma unroll
@@ -1149,19 +1154,20 @@ __global__ void __launch_bounds__(32 * kHeavyWarps) overlap_heavy_kernel(const Q
       lo[k] = p.queries[size_t(q) * 2 * D + k];
       hi[k] = p.queries[size_t(q) * 2 * D + D + k];
     }
-    if (lane == 0) s_fill[w] = p.fill ? p.csr_offsets[q] : 0ull;
-    uint32_t count = 0;
-    int sp = 0;
-    if (box_overlap<D>(p.root_box, p.root_box + D, lo, hi)) {
-      if (lane == 0) stk[0] = p.root_code;
-      sp = 1;
+    if (tid == 0) {
+      s_fill = p.fill ? p.csr_offsets[q] : 0ull;
+      const bool in_root = box_overlap<D>(p.root_box, p.root_box + D, lo, hi);
+      if (in_root) stk[0] = p.root_code;
+      s_sp = in_root ? 1 : 0;
     }
-    __syncwarp();
-    while (sp > 0) {
-      const int take = sp < 32 ? sp : 32;
-      const uint32_t code = lane < take ? stk[sp - take + lane] : kNoHit;
-      __syncwarp();
-      sp -= take;
+    uint32_t count = 0;
+    __syncthreads();
+    for (;;) {
+      const int sp = s_sp;
+      if (sp == 0) break;  // uniform: every thread read the same value
+      const int take = sp < T ? sp : T;
+      const uint32_t code = tid < take ? stk[sp - take + tid] : kNoHit;
+      __syncthreads();  // every entry taken is read before pushes overwrite it
       uint32_t push[2] = {kNoHit, kNoHit};
       if (code != kNoHit) {
         if (code & kLeafBit) {
@@ -1172,7 +1178,7 @@ __global__ void __launch_bounds__(32 * kHeavyWarps) overlap_heavy_kernel(const Q
             const uint32_t idw = __float_as_uint(rec[PL::id_word]);
             const uint32_t id = idw & ~kLeafBit;
             if (accepts(p, id) && narrow_overlap<D, N>(rec, lo, hi)) {
-              if (p.fill) p.csr_leaves[atomicAdd(&s_fill[w], 1ull)] = id;
+              if (p.fill) p.csr_leaves[atomicAdd(&s_fill, 1ull)] = id;
               else ++count;
             }
             if (idw & kLeafBit) break;
@@ -1185,6 +1191,8 @@ __global__ void __launch_bounds__(32 * kHeavyWarps) overlap_heavy_kernel(const Q
           if (box_overlap<D>(rec + 2 * D, rec + 3 * D, lo, hi)) push[1] = __float_as_uint(rec[4 * D + 1]);
         }
       }
+      // Block prefix sum of the children to push: within each warp, then
+      // across the warps' totals.
       const int mine = (push[0] != kNoHit) + (push[1] != kNoHit);
       int incl = mine;
 #pragma unroll
@@ -1192,23 +1200,39 @@ __global__ void __launch_bounds__(32 * kHeavyWarps) overlap_heavy_kernel(const Q
         const int v = __shfl_up_sync(FULL, incl, o);
         if (lane >= o) incl += v;
       }
-      const int total = __shfl_sync(FULL, incl, 31);
-      int at = sp + incl - mine;
+      if (lane == 31) s_wsum[w] = incl;
+      __syncthreads();
+      int before = 0, total = 0;
+#pragma unroll
+      for (int k = 0; k < kHeavyWarps; ++k) {
+        const int ws = s_wsum[k];
+        if (k < w) before += ws;
+        total += ws;
+      }
+      const int base = sp - take;
+      int at = base + before + incl - mine;
       for (int k = 0; k < 2; ++k) {
         if (push[k] == kNoHit) continue;
         if (at < cap) stk[at] = push[k];
         else atomicOr(p.heavy_count, 0x80000000u);  // refused: reported to the host
         ++at;
       }
-      sp = min(sp + total, cap);
-      __syncwarp();
+      __syncthreads();  // pushes written and s_wsum read before the next step
+      if (tid == 0) s_sp = min(base + total, cap);
+      __syncthreads();
     }
     if (!p.fill) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) count += __shfl_down_sync(FULL, count, o);
-      if (lane == 0) p.out_count[q] = count;
+      if (lane == 0) s_count[w] = count;
+      __syncthreads();
+      if (tid == 0) {
+        uint32_t c = 0;
+        for (int k = 0; k < kHeavyWarps; ++k) c += s_count[k];
+        p.out_count[q] = c;
+      }
     }
-    __syncwarp();
+    __syncthreads();  // the region's shared state is done before the next region's
   }
 }
 
@@ -1387,7 +1411,7 @@ struct KernelSet {
   const void* cast_nearest[2];    // [ref]
   const void* cast_all;
   const void* overlap;
-  const void* overlap_heavy;  // warp-per-region overlap of the regions over the visit budget
+  const void* overlap_heavy;  // block-per-region overlap of the regions over the visit budget
   const void* refit_leaves;
   const void* ray_nearest_seeded[2];  // [stats]; D = 3 only
 };
