@@ -779,10 +779,12 @@ size_t overlap_scan_temp(uint32_t n) {
 }
 
 // Scratch of overlap_core: per-region counts, the heavy-region list and
-// flags, their counter, then the scan's temporary storage.
+// flags, their counter, the count pass's kept leaves, then the scan's
+// temporary storage.
 size_t overlap_scratch_bytes(uint32_t n) {
   const auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
-  return al((size_t(n) + 1) * 4) + al(size_t(n) * 4 + 4) + al(size_t(n) + 1) + al(16) + overlap_scan_temp(n) + 256;
+  return al((size_t(n) + 1) * 4) + al(size_t(n) * 4 + 4) + al(size_t(n) + 1) + al(16) +
+         al(size_t(n) * kOverlapKeep * 4) + overlap_scan_temp(n) + 256;
 }
 
 // Records a region may visit before the block-per-region kernel takes it.
@@ -808,8 +810,9 @@ int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint3
   const auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
   Carve sc;
   const size_t o_cnt = sc.take((size_t(n) + 1) * 4), o_hl = sc.take(size_t(n) * 4 + 4), o_hf = sc.take(size_t(n) + 1),
-               o_hc = sc.take(16);
+               o_hc = sc.take(16), o_keep = sc.take(size_t(n) * kOverlapKeep * 4);
   (void)al;
+  uint32_t* d_keep = (uint32_t*)((char*)scratch + o_keep);
   uint32_t* d_counts = (uint32_t*)((char*)scratch + o_cnt);
   uint32_t* d_hlist = (uint32_t*)((char*)scratch + o_hl);
   uint8_t* d_hflag = (uint8_t*)((char*)scratch + o_hf);
@@ -827,6 +830,7 @@ int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint3
     p.n = n;
     p.out_count = d_counts;
     p.fill = 0;
+    p.keep = d_keep;
     if (heavy) {
       p.heavy_list = d_hlist;
       p.heavy_count = d_hcount;
@@ -857,6 +861,7 @@ int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint3
     p.fill = 2;
     p.csr_offsets = (const unsigned long long*)d_offsets;
     p.csr_leaves = d_leaves;
+    p.keep = d_keep;
     if (heavy) {
       p.heavy_list = d_hlist;
       p.heavy_count = d_hcount;

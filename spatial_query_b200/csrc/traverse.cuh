@@ -54,6 +54,9 @@ __device__ void sq_narrow_crossings(const float* prim, uint32_t leaf, const floa
 #endif
 enum QKind : int { kRayNearest = 0, kRayAll = 1, kCastNearest = 2, kCastAll = 3, kOverlap = 4 };
 
+// Leaves per region the overlap count pass keeps (QueryParams::keep).
+constexpr uint32_t kOverlapKeep = 4;
+
 constexpr int kThreads = 128;
 
 // Two walk variants, measured on the 1,048,576-triangle terrain and off by
@@ -276,6 +279,10 @@ struct QueryParams {
   uint32_t* heavy_count;
   uint8_t* heavy_flag;
   uint32_t visit_budget;
+  // Overlap: the count pass writes each region's first kOverlapKeep accepted
+  // leaves here ([n][kOverlapKeep]); the fill pass copies, sorted, the
+  // segment of every region with no more results instead of walking it again.
+  uint32_t* keep;
 };
 
 __device__ __forceinline__ bool accepts(const QueryParams& p, uint32_t id) {
@@ -686,6 +693,34 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
     if constexpr (K == kOverlap) {
       if (p.fill) L.csr_base = p.csr_offsets[q];
       if (p.fill && p.heavy_flag && p.heavy_flag[q]) return false;  // filled by the block-per-region kernel
+      if (p.fill && p.keep) {
+        // Every result of a region with at most kOverlapKeep of them was kept
+        // by the count pass (the same walk finds the same leaves): written
+        // ascending, with no second walk. Most regions have none.
+        const uint32_t c = uint32_t(p.csr_offsets[q + 1] - L.csr_base);
+        if (c <= kOverlapKeep) {
+          if (c) {
+            const uint4 k4 = __ldcs(reinterpret_cast<const uint4*>(p.keep) + q);
+            uint32_t v0 = k4.x, v1 = c > 1 ? k4.y : kNoHit, v2 = c > 2 ? k4.z : kNoHit, v3 = c > 3 ? k4.w : kNoHit;
+            const auto cas = [](uint32_t& a, uint32_t& b) {
+              const uint32_t lo = min(a, b);
+              b = max(a, b);
+              a = lo;
+            };
+            cas(v0, v1);  // sorting network on four: (0,1) (2,3) (0,2) (1,3) (1,2)
+            cas(v2, v3);
+            cas(v0, v2);
+            cas(v1, v3);
+            cas(v1, v2);
+            uint32_t* out = p.csr_leaves + L.csr_base;
+            out[0] = v0;
+            if (c > 1) out[1] = v1;
+            if (c > 2) out[2] = v2;
+            if (c > 3) out[3] = v3;
+          }
+          return false;
+        }
+      }
     }
     L.v_nodes = STATS ? 1u : 0u;
     L.v_nar = 0;
@@ -765,6 +800,7 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
       if (accepts(p, id)) {
         if constexpr (K == kOverlap) {
           if (narrow_overlap<D, N>(rec, L.r.o, L.r.d)) {
+            if (!p.fill && p.keep && L.count < kOverlapKeep) p.keep[size_t(L.q) * kOverlapKeep + L.count] = id;
             if (p.fill == 2) {
               // appended in walk order; a segmented sort orders each segment afterwards
               p.csr_leaves[L.csr_base + L.count] = id;
