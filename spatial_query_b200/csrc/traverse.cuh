@@ -274,7 +274,9 @@ struct QueryParams {
   int far_first;  // seeded walks: after the bucket, the crate's child order (push a, push b) instead of near-first
   // Overlap regions that visit more than visit_budget records in the count
   // pass are left to overlap_heavy_kernel (a block per region): listed in
-  // heavy_list, flagged in heavy_flag (the fill pass skips them).
+  // heavy_list, flagged in heavy_flag (1; the fill pass skips them). With
+  // keep set, the regions counted with more than kOverlapKeep results are
+  // listed too (flag 2) and filled by that kernel alone.
   uint32_t* heavy_list;
   uint32_t* heavy_count;
   uint8_t* heavy_flag;
@@ -642,7 +644,16 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
     } else if constexpr (kList) {
       p.out_count[q] = L.count;  // entries past min(count, k) are left as they were
     } else {
-      if (!p.fill) p.out_count[q] = L.count;
+      if (!p.fill) {
+        p.out_count[q] = L.count;
+        // A counted region with more results than the kept leaves (and not
+        // given up on) is filled by the block-per-region kernel too, so the
+        // fill pass walks no region again on one lane (flag 2: counted).
+        if (p.heavy_list && p.keep && L.count > kOverlapKeep && L.v_nar <= p.visit_budget) {
+          p.heavy_flag[q] = 2;
+          p.heavy_list[atomicAdd(p.heavy_count, 1u)] = q;
+        }
+      }
     }
     if (STATS) {
       c_vis += L.v_nodes;
@@ -1151,7 +1162,9 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
 }
 
 // ---------------------------------------------------------------------------
-// Heavy overlap regions: one block (128 threads) per region. The block keeps
+// Heavy overlap regions: one block (128 threads) per region, for the regions
+// the count pass gave up on (counted and filled here) and, in the fill pass,
+// for those it counted with more results than it kept. The block keeps
 // the region's pending nodes in one shared-memory stack and each step takes
 // up to 128 of them from the top, one per thread: an interior record's
 // overlapping children are pushed (block prefix sum for the slots), a leaf's
@@ -1184,6 +1197,7 @@ __global__ void __launch_bounds__(32 * kHeavyWarps) overlap_heavy_kernel(const Q
   const uint32_t nh = *p.heavy_count & 0x7FFFFFFFu;
   for (uint32_t i = blockIdx.x; i < nh; i += gridDim.x) {
     const uint32_t q = p.heavy_list[i];
+    if (!p.fill && p.heavy_flag[q] == 2) continue;  // counted by the count pass (uniform per block)
     float lo[D], hi[D];
 #pragma unroll
     for (int k = 0; k < D; ++k) {
