@@ -788,7 +788,7 @@ size_t overlap_scratch_bytes(uint32_t n) {
 }
 
 // Records a region may visit before the block-per-region kernel takes it.
-constexpr uint32_t kOverlapVisitBudget = 256;
+constexpr uint32_t kOverlapVisitBudget = 128;
 
 // Launches overlap_heavy_kernel over the regions the count pass listed (a
 // block per region, one shared stack of 256 x (depth + 1) entries).
