@@ -779,12 +779,13 @@ size_t overlap_scan_temp(uint32_t n) {
 }
 
 // Scratch of overlap_core: per-region counts, the heavy-region list and
-// flags, their counter, the count pass's kept leaves, then the scan's
-// temporary storage.
+// flags, their counter and store cursor, the count pass's kept leaves, the
+// heavy regions' staged-leaf slots and store (n entries each), then the
+// scan's temporary storage.
 size_t overlap_scratch_bytes(uint32_t n) {
   const auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
   return al((size_t(n) + 1) * 4) + al(size_t(n) * 4 + 4) + al(size_t(n) + 1) + al(16) +
-         al(size_t(n) * kOverlapKeep * 4) + overlap_scan_temp(n) + 256;
+         al(size_t(n) * kOverlapKeep * 4) + 2 * al(size_t(n) * 4 + 4) + overlap_scan_temp(n) + 256;
 }
 
 // Records a region may visit before the block-per-region kernel takes it.
@@ -796,7 +797,7 @@ int32_t launch_heavy(sq_ctx* ctx, const sq_bvh* b, QueryParams& p) {
   const uint32_t cap = 256u * (b->depth + 1);
   p.stack = int(cap);
   const size_t smem = size_t(cap) * 4;
-  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(b->ks.overlap_heavy, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  if (smem + kHeavyStage * 4 + 1024 > 48 * 1024) CK(cudaFuncSetAttribute(b->ks.overlap_heavy, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   void* args[] = {&p};
   CK(cudaLaunchKernel(b->ks.overlap_heavy, dim3(ctx->sm_count * 4), dim3(32 * kHeavyWarps), args, smem, ctx->stream));
   ctx->launches++;
@@ -810,9 +811,12 @@ int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint3
   const auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
   Carve sc;
   const size_t o_cnt = sc.take((size_t(n) + 1) * 4), o_hl = sc.take(size_t(n) * 4 + 4), o_hf = sc.take(size_t(n) + 1),
-               o_hc = sc.take(16), o_keep = sc.take(size_t(n) * kOverlapKeep * 4);
+               o_hc = sc.take(16), o_keep = sc.take(size_t(n) * kOverlapKeep * 4),
+               o_hst = sc.take(size_t(n) * 4 + 4), o_hsto = sc.take(size_t(n) * 4 + 4);
   (void)al;
   uint32_t* d_keep = (uint32_t*)((char*)scratch + o_keep);
+  uint32_t* d_hstart = (uint32_t*)((char*)scratch + o_hst);
+  uint32_t* d_hstore = (uint32_t*)((char*)scratch + o_hsto);
   uint32_t* d_counts = (uint32_t*)((char*)scratch + o_cnt);
   uint32_t* d_hlist = (uint32_t*)((char*)scratch + o_hl);
   uint8_t* d_hflag = (uint8_t*)((char*)scratch + o_hf);
@@ -821,7 +825,8 @@ int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint3
   size_t temp_bytes = scratch_bytes - sc.off;
   CK(cudaMemsetAsync(d_counts, 0, size_t(n + 1) * 4, ctx->stream));
   CK(cudaMemsetAsync(d_hflag, 0, size_t(n) + 1, ctx->stream));
-  CK(cudaMemsetAsync(d_hcount, 0, 4, ctx->stream));
+  CK(cudaMemsetAsync(d_hcount, 0, 8, ctx->stream));  // list count, store cursor
+  CK(cudaMemsetAsync(d_hstart, 0xFF, size_t(n) * 4, ctx->stream));
   const bool heavy = b->ks.overlap_heavy != nullptr;
   if (b->n_nodes != 0 && n != 0) {
     QueryParams p;
@@ -836,6 +841,10 @@ int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint3
       p.heavy_count = d_hcount;
       p.heavy_flag = d_hflag;
       p.visit_budget = kOverlapVisitBudget;
+      p.heavy_store = d_hstore;
+      p.heavy_start = d_hstart;
+      p.heavy_cursor = d_hcount + 1;
+      p.heavy_cap = n;
     }
     int32_t rc = launch_persistent(ctx, b->ks.overlap, p, b->depth, p.n);
     if (rc) return rc;
@@ -866,6 +875,8 @@ int32_t overlap_core(sq_ctx* ctx, const sq_bvh* b, const float* d_regions, uint3
       p.heavy_list = d_hlist;
       p.heavy_count = d_hcount;
       p.heavy_flag = d_hflag;
+      p.heavy_store = d_hstore;
+      p.heavy_start = d_hstart;
     }
     int32_t rc = launch_persistent(ctx, b->ks.overlap, p, b->depth, p.n);
     if (rc) return rc;

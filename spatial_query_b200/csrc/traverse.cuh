@@ -285,6 +285,11 @@ struct QueryParams {
   // leaves here ([n][kOverlapKeep]); the fill pass copies, sorted, the
   // segment of every region with no more results instead of walking it again.
   uint32_t* keep;
+  // Overlap: overlap_heavy_kernel's staged leaves (see that kernel).
+  uint32_t* heavy_store;
+  uint32_t* heavy_start;   // per heavy_list entry
+  uint32_t* heavy_cursor;
+  uint32_t heavy_cap;      // entries of heavy_store
 };
 
 __device__ __forceinline__ bool accepts(const QueryParams& p, uint32_t id) {
@@ -1178,8 +1183,14 @@ __global__ void __launch_bounds__(kThreads) query_kernel(const QueryParams p) {
 // top: it never holds more than 128 x (depth + 2) entries; it is sized
 // 256 x (depth + 1) (dynamic shared memory), and a push past it is refused
 // and reported through heavy_count's high bit instead of written.
+// With heavy_store set, the count pass also stages a region's leaves in
+// shared memory (up to kHeavyStage) and copies them to heavy_store at a
+// slot taken from heavy_cursor (heavy_start[i]: the slot, kNoHit when the
+// stage or the store was too small); the fill pass then copies that region's
+// segment from there instead of walking it again.
 // ---------------------------------------------------------------------------
 constexpr int kHeavyWarps = 4;
+constexpr uint32_t kHeavyStage = 2048;
 
 template <int D, int N>
 __global__ void __launch_bounds__(32 * kHeavyWarps) overlap_heavy_kernel(const QueryParams p) {
@@ -1191,13 +1202,25 @@ __global__ void __launch_bounds__(32 * kHeavyWarps) overlap_heavy_kernel(const Q
   __shared__ unsigned long long s_fill;
   __shared__ int s_sp;
   __shared__ int s_wsum[kHeavyWarps];
-  __shared__ uint32_t s_count[kHeavyWarps];
+  __shared__ uint32_t s_n;      // the region's accepted leaves so far
+  __shared__ uint32_t s_start;  // its slot in heavy_store (kNoHit: none)
+  __shared__ uint32_t s_stage[kHeavyStage];
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   const int cap = p.stack;  // entries
   const uint32_t nh = *p.heavy_count & 0x7FFFFFFFu;
   for (uint32_t i = blockIdx.x; i < nh; i += gridDim.x) {
     const uint32_t q = p.heavy_list[i];
     if (!p.fill && p.heavy_flag[q] == 2) continue;  // counted by the count pass (uniform per block)
+    if (p.fill && p.heavy_start) {
+      const uint32_t st = p.heavy_start[i];  // uniform per block
+      if (st != kNoHit) {
+        // staged by the count pass: a copy, no second walk
+        const unsigned long long base = p.csr_offsets[q];
+        const uint32_t c = uint32_t(p.csr_offsets[q + 1] - base);
+        for (uint32_t k = tid; k < c; k += T) p.csr_leaves[base + k] = p.heavy_store[st + k];
+        continue;
+      }
+    }
     float lo[D], hi[D];
 #pragma unroll
     for (int k = 0; k < D; ++k) {
@@ -1206,11 +1229,11 @@ __global__ void __launch_bounds__(32 * kHeavyWarps) overlap_heavy_kernel(const Q
     }
     if (tid == 0) {
       s_fill = p.fill ? p.csr_offsets[q] : 0ull;
+      s_n = 0;
       const bool in_root = box_overlap<D>(p.root_box, p.root_box + D, lo, hi);
       if (in_root) stk[0] = p.root_code;
       s_sp = in_root ? 1 : 0;
     }
-    uint32_t count = 0;
     __syncthreads();
     for (;;) {
       const int sp = s_sp;
@@ -1228,8 +1251,12 @@ __global__ void __launch_bounds__(32 * kHeavyWarps) overlap_heavy_kernel(const Q
             const uint32_t idw = __float_as_uint(rec[PL::id_word]);
             const uint32_t id = idw & ~kLeafBit;
             if (accepts(p, id) && narrow_overlap<D, N>(rec, lo, hi)) {
-              if (p.fill) p.csr_leaves[atomicAdd(&s_fill, 1ull)] = id;
-              else ++count;
+              if (p.fill) {
+                p.csr_leaves[atomicAdd(&s_fill, 1ull)] = id;
+              } else {
+                const uint32_t k = atomicAdd(&s_n, 1u);
+                if (k < kHeavyStage) s_stage[k] = id;
+              }
             }
             if (idw & kLeafBit) break;
             ++pos;
@@ -1272,15 +1299,22 @@ __global__ void __launch_bounds__(32 * kHeavyWarps) overlap_heavy_kernel(const Q
       __syncthreads();
     }
     if (!p.fill) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) count += __shfl_down_sync(FULL, count, o);
-      if (lane == 0) s_count[w] = count;
-      __syncthreads();
+      // The walk's last step ended at a barrier: s_n is final.
+      const uint32_t c = s_n;
       if (tid == 0) {
-        uint32_t c = 0;
-        for (int k = 0; k < kHeavyWarps; ++k) c += s_count[k];
         p.out_count[q] = c;
+        uint32_t st = kNoHit;
+        if (p.heavy_start && c <= kHeavyStage) {
+          const uint32_t at = atomicAdd(p.heavy_cursor, c);
+          if (at <= p.heavy_cap && c <= p.heavy_cap - at) st = at;
+        }
+        s_start = st;
+        if (p.heavy_start) p.heavy_start[i] = st;
       }
+      __syncthreads();
+      const uint32_t st = s_start;
+      if (st != kNoHit)
+        for (uint32_t k = tid; k < c; k += T) p.heavy_store[st + k] = s_stage[k];
     }
     __syncthreads();  // the region's shared state is done before the next region's
   }
