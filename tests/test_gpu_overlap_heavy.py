@@ -1,8 +1,10 @@
-"""Overlap regions heavier than the per-thread visit budget are finished by
-the warp-per-region kernel; the CSR result (offsets, and each region's
-leaves ascending) must equal the oracle's whatever mix of light and heavy
-regions a batch holds: regions covering most of a box scene among small
-ones, with a layer filter, in 3 and 6 dimensions, and through the
+"""Overlap regions heavier than the per-thread visit budget, and regions
+with more results than the count pass keeps, are finished by the
+block-per-region kernel (its count pass stores the leaves it finds, its fill
+pass copies them or walks again); the CSR result (offsets, and each
+region's leaves ascending) must equal the oracle's whatever mix of light
+and heavy regions a batch holds: regions covering most of a box scene among
+small ones, with a layer filter, in 3 and 6 dimensions, and through the
 host-buffer and device-pointer calls."""
 import numpy as np
 import pytest
